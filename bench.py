@@ -1,0 +1,298 @@
+#!/usr/bin/env python
+"""Throughput of the explicit Heun path (cell-updates/s) on B200.
+
+Workload: the scaled square4 layout -- 4 blocks of 1024 x 1024 cells tiling
+[-1,1]^2 (4,194,304 cells, 9 FP64 moments each), open (extrapolation) outer
+edges, seeded quadrant initial state (rho, theta ~ U[0.5,2], vx, vy ~
+U[-0.3,0.3]), Kn = 0.01, R13 = 1, harmonic limiter, CFL 0.95.  A step is one
+accepted Heun step (two stages, two ghost fills, the dt controller); cell-updates
+= cells x accepted steps, the reference's own measure (src/tools.c:87-95,
+src/Main.c:223).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line on rank 0.  Under torchrun each rank advances its own
+replica of the workload (weak scaling, no collective on the data path); the
+time is the max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s"
+BYTES_PER_CELL_UPDATE = 360          # stage 1: 72 read + 72 write; stage 2: 144 read + 72 write
+STAGE_BYTES = (144, 216)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def workload(n, seed):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import helpers as H
+    from multiblockmomentsfv_b200 import scenario as sc
+    d = H.quadrant_deck(n, Kn=0.01, R13=1.0)
+    return d, sc.Scenario.seeded_quadrant(seed)
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                out, _ = self.p.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference(steps, warmup, budget, n=0, threads=None):
+    cmd = [sys.executable, os.path.join(ROOT, "oracle", "ref_bench.py"), "--steps", str(steps),
+           "--warmup", str(warmup), "--budget", str(budget), "--threads", str(threads or os.cpu_count() or 1)]
+    if n:
+        cmd += ["--n", str(n)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        return {"unavailable": (r.stderr.strip().splitlines() or ["ref_bench failed"])[-1]}
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def run_reference(a, rank):
+    if rank != 0:
+        return
+    budget = max(30.0, min(150.0, 1.5 * (a.steps + a.warmup)))
+    r = cpu_reference(a.steps, a.warmup, budget)
+    if "unavailable" in r:
+        print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
+        return
+    sample = (f"{r['steps']} accepted Heun steps (after {a.warmup} warm-up) of the same layout at "
+              f"{r['n']}x{r['n']} cells per block ({r['cells']} cells): the reference's TimeUpdate "
+              f"({r['build']}, OpenMP over the 4 blocks) driven by its Steps controller")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "cell-updates/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * r["seconds"] / max(1, r["steps"]), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "scaled square4, 4 blocks, seeded quadrant state, Kn=0.01, harmonic, CFL 0.95, "
+                               "FP64; bounded sample of the 4 x 1024^2 grid", "n_per_block": r["n"],
+                   "cells": r["cells"]},
+        "cpu_baseline": {"value": r["value"], "unit": "cell-updates/s", "cores": r["cores"],
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": r["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=1024, help="cells per block side")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--e2e-calls", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=50, help="Heun steps per Steps() call in the e2e leg")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--segment-rows", type=int, default=0)
+    a = ap.parse_args()
+    if a.warmup < 3:
+        a.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference(a, rank)
+        return
+
+    import torch
+    import numpy as np
+    from multiblockmomentsfv_b200 import solver as sv
+    import datetime
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    d, scn = workload(a.n, a.seed + rank)
+    cells = d.full_grid_size
+    stream = torch.cuda.Stream()
+    s = sv.Solver(d, scn, device=local, show_every=0, stream=stream.cuda_stream,
+                  segment_rows=a.segment_rows)
+    s.initialise()
+    t, n0, _ = s.steps(0.0, 0.3, max_steps=a.warmup)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        t, nsteps, nrej = s.steps(t, 0.3, max_steps=a.steps)
+        e1.record(stream)
+        stream.synchronize()
+    attempts = s.attempts()
+    ms = e0.elapsed_time(e1)
+    barrier()
+    ms_max = ms
+    if dist:
+        v = torch.tensor([ms, float(nsteps)], device="cuda")
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        ms_max = float(v[0])
+        tot = torch.tensor([float(nsteps)], device="cuda")
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        total_updates = cells * float(tot[0])
+    else:
+        total_updates = cells * nsteps
+    value = total_updates / (ms_max / 1e3)
+
+    # dominant kernel: the stage kernel, timed alone with CUDA events (both Heun flags)
+    dt = 1e-4
+    ms1 = s.time_stage(0, dt, reps=5)
+    ms2 = s.time_stage(1, dt, reps=5)
+    achieved = BYTES_PER_CELL_UPDATE * cells / ((ms1 + ms2) / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tj = json.load(f)
+        if tj.get("cells_per_launch"):
+            traffic = tj["dram_bytes_per_launch_per_cell"] * cells
+
+    # end to end through the C ABI with host buffers: upload DATA (pinned host, array of
+    # structs), one Steps() call of e2e-steps Heun steps, download DATA -- per call
+    host = [torch.empty((b.nyp, b.nxp, 9), dtype=torch.float64, pin_memory=True) for b in d.blocks]
+    for b in range(len(d.blocks)):
+        s.download(0, b, host[b].numpy())
+    h2d = sum(x.numel() * 8 for x in host)
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = 0
+    f0.record(stream)
+    for _ in range(a.e2e_calls):
+        for b in range(len(d.blocks)):
+            s.upload(0, b, host[b].numpy())
+        t, nn, _ = s.steps(t, 0.3, max_steps=a.e2e_steps)
+        e2e_steps += nn
+        for b in range(len(d.blocks)):
+            s.download(0, b, host[b].numpy())
+    f1.record(stream)
+    stream.synchronize()
+    ms_e2e = f0.elapsed_time(f1)
+    if dist:
+        v = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        ms_e2e = float(v[0])
+    e2e_value = world * cells * e2e_steps / (ms_e2e / 1e3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        r = cpu_reference(3, 0, 20.0, n=0)
+        if "unavailable" not in r:
+            cpu = {"value": r["value"], "unit": "cell-updates/s", "cores": r["cores"], "kind": "reference",
+                   "sample": f"{r['steps']} Heun steps of the same layout at {r['n']}x{r['n']} cells per block "
+                             f"({r['cells']} cells), the reference's TimeUpdate ({r['build']}, "
+                             f"{r['threads']} threads, OpenMP over 4 blocks), this host"}
+        else:
+            cpu = {"unavailable": r["unavailable"]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": nsteps, "warmup": a.warmup, "ms_per_step": ms_max / max(1, nsteps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": f"synthetic: seeded quadrant state (seed {a.seed}+rank)",
+            "config": {"workload": f"scaled square4: 4 blocks x {a.n}^2 cells ({cells} cells), open outer "
+                                   "edges, Kn=0.01, R13=1, harmonic, CFL 0.95, FP64, bitwise mode",
+                       "cells": cells, "rejected_attempts": nrej,
+                       "l2": "working set 3 layers x 4 blocks x 9 planes = "
+                             f"{3 * 9 * 8 * sum(b.cells for b in d.blocks) / 1e6:.0f} MB > 126 MB L2, no flush",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "stage_kernel (Heun stage 1 + stage 2)",
+                         "ms_per_launch": [ms1, ms2],
+                         "algorithmic_bytes_per_launch": [STAGE_BYTES[0] * cells, STAGE_BYTES[1] * cells]},
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": h2d / max(1, a.e2e_steps),
+                    "d2h_bytes_per_step": h2d / max(1, a.e2e_steps),
+                    "steps_per_call": a.e2e_steps, "calls": a.e2e_calls},
+            "gpu_launches": 5 * attempts,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

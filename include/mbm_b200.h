@@ -1,0 +1,140 @@
+/*
+ * mbm_b200.h -- C ABI of the B200 (sm_100a) implementation of MultiBlockMomentsFV's
+ * explicit Heun time-stepping path.
+ *
+ * The reference has no plugin layer: its hot path is the C function
+ *     int Steps(DB_Block *B, int bMax, double *t, double tend, double CFLmax, double CFLreg)
+ * (src/Main.c:31,189-244) with TimeUpdate (src/Main.c:253-284), Update
+ * (src/Main.c:297-396) and SetBoundary (src/Boundary.c:173-193) below it, reading
+ * the globals Kn, F (src/Scenario.c:22-23) and Limiter (src/Limiter.c:20).  The
+ * entry points below replace those functions one for one; the host keeps its own
+ * DB_Block arrays (array of structs, 9 doubles per cell, x fastest, ghosts
+ * included) and passes them as plain pointers.
+ *
+ * Every call returns an int status (MBM_OK = 0).  No exception crosses the ABI.
+ * A context is not thread-safe; use one host thread per context.
+ */
+#ifndef MBM_B200_H
+#define MBM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MBM_OK          0
+#define MBM_EINVAL      1   /* bad argument or block table                       */
+#define MBM_ENONFINITE  2   /* CFL or dt became non-finite / non-positive         */
+#define MBM_ETIMEOUT    3   /* a bounded host wait on the device ran out          */
+#define MBM_ECUDA       4   /* a CUDA runtime call failed (see mbm_last_error)   */
+#define MBM_ENOMEM      5   /* device allocation failed                          */
+#define MBM_ESTEPLIMIT  6   /* step attempts exceeded max_attempts               */
+#define MBM_ENODEV      7   /* no CUDA device                                    */
+
+/* layers, as the reference's layer enum (src/defs.h:21-24) */
+#define MBM_L_DATA 0
+#define MBM_L_TMP  1
+#define MBM_L_NEW  2
+
+/* limiters, as src/Limiter.h:9-15 */
+#define MBM_LIM_NONE     0
+#define MBM_LIM_AVERAGE  1
+#define MBM_LIM_MINMOD   2
+#define MBM_LIM_SUPERBEE 3
+#define MBM_LIM_HARMONIC 4
+
+/* arithmetic modes */
+#define MBM_MODE_EXACT 0   /* operation-for-operation the reference: bitwise-equal results */
+
+/* One block: the DB_Block fields the path reads (src/defs.h:59-68). */
+typedef struct {
+  int nx, ny;          /* interior cells; the block holds (nx+6)*(ny+6) cells       */
+  double x0, y0;       /* centre of padded cell (0,0): B.x, B.y (src/Mesh.c:364-365) */
+  double dx, dy;
+  int bc[4];           /* left, right, bottom, top: >0 sync with block code,
+                          0 open, -1 wall, -2 Dirichlet (src/defs.h:26-31)          */
+} mbm_block_desc;
+
+typedef struct {
+  double Kn;           /* Knudsen number (collision frequency rho*sqrt(theta)/Kn)   */
+  double F;            /* body force in x                                          */
+  int limiter;         /* MBM_LIM_*                                                */
+  int mode;            /* MBM_MODE_*                                               */
+  int device;          /* CUDA device ordinal                                      */
+  int show_every;      /* progress record every n accepted steps (reference: 20); 0 = none */
+  int max_attempts;    /* bound on step attempts per mbm_steps call; 0 = 10,000,000 */
+  int segment_rows;    /* rows per warp work item; 0 = tuned default               */
+  void *stream;        /* cudaStream_t to launch on; NULL = a stream the context owns */
+} mbm_params;
+
+typedef struct mbm_ctx mbm_ctx;
+
+/* Allocate device state for a block table.  Replaces the allocation in main()
+ * (src/Main.c:113-123).  Sync partners must have equal tangential extents
+ * (src/Boundary.c:101-103) and codes must name existing blocks. */
+int mbm_create(const mbm_block_desc *blocks, int nblocks, const mbm_params *params, mbm_ctx **ctx);
+int mbm_destroy(mbm_ctx *ctx);
+
+/* Copy one block of a layer between the host (array of structs, (nx+6)*(ny+6)*9
+ * doubles, the reference's CVector layer, src/defs.h:42-44) and the device. */
+int mbm_upload(mbm_ctx *ctx, int layer, int block, const double *cells);
+int mbm_download(mbm_ctx *ctx, int layer, int block, double *cells);
+
+/* Dirichlet ghost values of one edge (code -2), in FillEdge's order: tangential
+ * index over the full edge, corners included, outer; ghost layer n = 1..3 inner
+ * (src/Boundary.c:105-129); 9 doubles each.  The host evaluates its SetInitial
+ * at each ghost centre (src/Boundary.c:127-129); the values hold until set again. */
+int mbm_set_dirichlet(mbm_ctx *ctx, int block, int side, const double *values);
+
+/* SetBoundary (src/Boundary.c:173-193) on one layer. */
+int mbm_set_boundary(mbm_ctx *ctx, int layer, double t);
+
+/* Update (src/Main.c:297-396) of every block: out_layer <- stage(in_layer),
+ * Data0 = data0_layer, Heun flag heun; cfl[b] receives each block's return value
+ * (may be NULL). */
+int mbm_update(mbm_ctx *ctx, int out_layer, int in_layer, int data0_layer, double dt, double t,
+               int heun, double *cfl);
+
+/* TimeUpdate (src/Main.c:253-284): both Heun stages with a boundary fill after
+ * each; *cfl receives max over stages and blocks. */
+int mbm_time_update(mbm_ctx *ctx, double dt, double t, double *cfl);
+
+/* Steps (src/Main.c:189-244): advance DATA from *t to tend with the a-posteriori
+ * CFL control (reject if CFL > CFLmax, next dt = dt*CFLreg/CFL, dt restarts at
+ * 1e-4 on every call).  The step loop runs on the device (a CUDA graph with a
+ * conditional while node); the host waits once.  *nsteps = accepted steps,
+ * *nrej = rejected attempts (either may be NULL). */
+int mbm_steps(mbm_ctx *ctx, double *t, double tend, double CFLmax, double CFLreg, int *nsteps,
+              int *nrej);
+
+/* mbm_steps with a cap on accepted steps (max_steps > 0); the loop also ends at
+ * tend.  Used for fixed-length runs (benchmarks, the many-case workloads). */
+int mbm_steps_capped(mbm_ctx *ctx, double *t, double tend, double CFLmax, double CFLreg,
+                     int max_steps, int *nsteps, int *nrej);
+
+/* Device time of the stage kernel alone: `reps` launches of Heun stage `heun` on
+ * the current layers (TMP <- DATA, or NEW <- TMP with Data0 = DATA) at step dt,
+ * bracketed by CUDA events on the context's stream.  *ms = mean per launch. */
+int mbm_time_stage(mbm_ctx *ctx, int heun, double dt, int reps, double *ms);
+
+/* Progress records of the last mbm_steps call, one per show_every accepted steps:
+ * {step, CFL, t, next dt}, the values the reference prints (src/Main.c:218-230). */
+int mbm_trace(mbm_ctx *ctx, double *records, int cap, int *n);
+
+/* Step attempts (accepted + rejected) of the last mbm_steps call; each attempt
+ * runs five kernels (two stages, two ghost fills, the controller). */
+int mbm_attempts(mbm_ctx *ctx, int *attempts);
+
+/* Host-only: the resolved ghost-cell sources of a block table, 4 ints per ghost
+ * cell {dst_block, dst_cell, src, src_block | flags<<16}; cells are J*(nx+6)+I,
+ * src < 0 is Dirichlet row -(src+1), flags bit 0/1 = x/y wall sign.  Needs no GPU. */
+int mbm_ghost_map(const mbm_block_desc *blocks, int nblocks, int *entries, int cap, int *n);
+
+const char *mbm_strerror(int status);
+/* last CUDA / validation message of a context (or the last mbm_create failure when ctx is NULL) */
+const char *mbm_last_error(mbm_ctx *ctx);
+int mbm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,100 @@
+"""ctypes binding of the C ABI declared in include/mbm_b200.h.
+
+The shared library is built in place by ``multiblockmomentsfv_b200.build``.  There
+is no fallback: if the library is missing or a call fails, a ``MBMError`` is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import build as _build
+
+MBM_OK, MBM_EINVAL, MBM_ENONFINITE, MBM_ETIMEOUT, MBM_ECUDA, MBM_ENOMEM, MBM_ESTEPLIMIT, MBM_ENODEV = range(8)
+L_DATA, L_TMP, L_NEW = 0, 1, 2
+MODE_EXACT = 0
+
+# every symbol include/mbm_b200.h declares
+EXPORTS = (
+    "mbm_create", "mbm_destroy", "mbm_upload", "mbm_download", "mbm_set_dirichlet",
+    "mbm_set_boundary", "mbm_update", "mbm_time_update", "mbm_steps", "mbm_steps_capped",
+    "mbm_time_stage", "mbm_trace", "mbm_attempts",
+    "mbm_ghost_map", "mbm_strerror", "mbm_last_error", "mbm_version",
+)
+
+
+class BlockDesc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("x0", C.c_double), ("y0", C.c_double),
+                ("dx", C.c_double), ("dy", C.c_double), ("bc", C.c_int * 4)]
+
+
+class Params(C.Structure):
+    _fields_ = [("Kn", C.c_double), ("F", C.c_double), ("limiter", C.c_int), ("mode", C.c_int),
+                ("device", C.c_int), ("show_every", C.c_int), ("max_attempts", C.c_int),
+                ("segment_rows", C.c_int), ("stream", C.c_void_p)]
+
+
+class MBMError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+_lib = None
+
+
+def lib(path: str = None):
+    """Load the library (building it first if it is missing or stale)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if path is None:
+        path = _build.LIB
+        if not os.path.exists(path):
+            _build.build()
+    L = C.CDLL(path)
+    P = C.POINTER
+    dp = P(C.c_double)
+    vp = C.c_void_p
+    L.mbm_create.argtypes = [P(BlockDesc), C.c_int, P(Params), P(vp)]
+    L.mbm_destroy.argtypes = [vp]
+    L.mbm_upload.argtypes = [vp, C.c_int, C.c_int, dp]
+    L.mbm_download.argtypes = [vp, C.c_int, C.c_int, dp]
+    L.mbm_set_dirichlet.argtypes = [vp, C.c_int, C.c_int, dp]
+    L.mbm_set_boundary.argtypes = [vp, C.c_int, C.c_double]
+    L.mbm_update.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, dp]
+    L.mbm_time_update.argtypes = [vp, C.c_double, C.c_double, dp]
+    L.mbm_steps.argtypes = [vp, dp, C.c_double, C.c_double, C.c_double, P(C.c_int), P(C.c_int)]
+    L.mbm_steps_capped.argtypes = [vp, dp, C.c_double, C.c_double, C.c_double, C.c_int, P(C.c_int),
+                                   P(C.c_int)]
+    L.mbm_time_stage.argtypes = [vp, C.c_int, C.c_double, C.c_int, dp]
+    L.mbm_trace.argtypes = [vp, dp, C.c_int, P(C.c_int)]
+    L.mbm_attempts.argtypes = [vp, P(C.c_int)]
+    L.mbm_ghost_map.argtypes = [P(BlockDesc), C.c_int, P(C.c_int), C.c_int, P(C.c_int)]
+    L.mbm_strerror.restype = C.c_char_p
+    L.mbm_strerror.argtypes = [C.c_int]
+    L.mbm_last_error.restype = C.c_char_p
+    L.mbm_last_error.argtypes = [vp]
+    for name in EXPORTS:
+        getattr(L, name).restype = getattr(L, name).restype or C.c_int
+    L.mbm_strerror.restype = C.c_char_p
+    L.mbm_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def check(status: int, ctx=None) -> None:
+    if status != MBM_OK:
+        L = lib()
+        msg = L.mbm_last_error(ctx).decode() or L.mbm_strerror(status).decode()
+        raise MBMError(status, msg)
+
+
+def block_descs(blocks):
+    arr = (BlockDesc * len(blocks))()
+    for i, b in enumerate(blocks):
+        arr[i].nx, arr[i].ny = b.nx, b.ny
+        arr[i].x0, arr[i].y0, arr[i].dx, arr[i].dy = b.x0, b.y0, b.dx, b.dy
+        for s in range(4):
+            arr[i].bc[s] = b.bc[s]
+    return arr

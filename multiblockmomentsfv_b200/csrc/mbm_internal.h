@@ -1,0 +1,72 @@
+// mbm_internal.h -- device data structures shared by the kernels and the host side.
+//
+// HBM layout (one allocation per physical layer): every block stores its nine
+// moments as nine planes (structure of arrays) of nyp rows x pitch doubles, with
+// cell (I, J) of the padded grid (I, J = 0 .. nxp-1 / nyp-1, ghosts included) at
+// element J*pitch + I + 1.  The leading pad column puts the first column a warp
+// strip reads (I0 - 2, with I0 = 1 + 28k) on a 32-byte sector boundary; pitch is a
+// multiple of 4 doubles so every row starts on one too.
+//
+// Physical layers: buf[0], buf[1] hold DATA and NEW, swapped by index when a step
+// is accepted (the reference copies NEW into DATA, src/Main.c:236-240); buf[2] is
+// TMP.  Each case keeps the index of its DATA buffer in CaseDev::cur.
+#pragma once
+
+#include <stdint.h>
+
+namespace mbm {
+
+constexpr int NV = 9;           // moments per cell (src/defs.h:11)
+constexpr int NG = 3;           // ghost layers per edge (src/defs.h:14)
+constexpr int STRIP = 28;        // output columns per warp strip (32 lanes - 2 - 2 halo)
+constexpr int MAX_TRACE = 4096;  // progress records kept per case and Steps call
+
+enum LayerSel : int { SEL_CUR = 0, SEL_OTHER = 1, SEL_TMP = 2 };
+
+struct BlockDev {
+  int nxp, nyp;        // padded extents (nx+6, ny+6)
+  int pitch;           // row stride in doubles
+  int case_id;
+  long long off;       // element offset of the block's first plane in a layer buffer
+  long long plane;     // elements per moment plane
+  double dx, dy;
+};
+
+struct Work {          // one warp strip segment: columns [I0, I0+28), face rows [J0, J1)
+  int blk, I0, J0, J1;
+};
+
+struct GhostEntry {    // final value of one ghost cell after the two-sweep fill
+  int dst_blk;
+  int dst;             // element index (J*pitch + I + 1) in block dst_blk
+  int src;             // >= 0: element index in block src_blk; < 0: Dirichlet row -(src+1)
+  int src_blk_flags;   // src_blk | (x-wall flip << 16) | (y-wall flip << 17)
+};
+
+struct CaseDev {       // per-case step controller (src/Main.c:189-244)
+  double t, tend, dt, CFLmax, CFLreg, Kn, F;
+  double cfl_last;
+  int limiter, cur;
+  int nstep, nrej, attempts, max_attempts, step_cap;
+  int done, status;
+  int show_every, trace_n;
+  int blk0, nblk;      // the case's blocks are blk0 .. blk0+nblk-1
+  int pad_;
+};
+
+struct StageArgs {
+  const BlockDev* blk;
+  const Work* work;
+  int nwork;
+  CaseDev* cases;
+  double* buf[3];
+  unsigned long long* lam;   // [block][stage][3]: max lambda_x, lambda_y, CFL_prod bits
+  int sel_in, sel_d0, sel_out;
+  int heun;
+};
+
+__host__ __device__ inline int phys_layer(int sel, int cur) {
+  return sel == SEL_CUR ? cur : (sel == SEL_OTHER ? 1 - cur : 2);
+}
+
+}  // namespace mbm

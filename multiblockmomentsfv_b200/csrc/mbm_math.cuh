@@ -1,0 +1,222 @@
+// mbm_math.cuh -- per-cell and per-face FP64 arithmetic of the Grad-13 Heun stage.
+//
+// Bitwise mode: every expression keeps the operand order and association of the
+// reference expression it restates (file:line cited per function), the file is
+// compiled with -fmad=false, and double division and sqrt are IEEE round-to-
+// nearest on sm_100a, so results agree bit for bit with the reference compiled
+// by gcc on x86-64 (SSE2, no contraction).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "mbm_internal.h"
+
+namespace mbm {
+
+// the reference's max/min/sgn (src/tools.h:3-17): a > b ? a : b etc.
+__device__ __forceinline__ double rmax(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double rmin(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double rsgn(double a) { return a == 0 ? 0.0 : (a < 0 ? -1.0 : 1.0); }
+
+// Primitive (src/Flux.c:30-56)
+__device__ __forceinline__ void primitive(const double (&U)[NV], double (&P)[NV]) {
+  const double rho = U[0];
+  const double v1 = U[1] / rho, v2 = U[2] / rho;
+  const double vs = v1 * v1 + v2 * v2;
+  const double th = (2 * U[3] / rho - vs) / 3;
+  const double E = U[3];
+  const double T11 = U[4] / rho - v1 * v1;
+  const double T12 = U[5] / rho - v1 * v2;
+  const double T22 = U[6] / rho - v2 * v2;
+  P[0] = rho; P[1] = v1; P[2] = v2; P[3] = th;
+  P[4] = T11; P[5] = T12; P[6] = T22;
+  P[7] = U[7] - E * v1 - rho * (T11 * v1 + T12 * v2);
+  P[8] = U[8] - E * v2 - rho * (T12 * v1 + T22 * v2);
+}
+
+// moments with an explicit energy (src/Flux.c:65-73, 255-263)
+__device__ __forceinline__ void moments_e(double rho, double v1, double v2, double E, double T11,
+                                          double T12, double T22, double q1, double q2,
+                                          double (&U)[NV]) {
+  U[0] = rho;
+  U[1] = rho * v1;
+  U[2] = rho * v2;
+  U[3] = E;
+  U[4] = rho * (T11 + v1 * v1);
+  U[5] = rho * (T12 + v1 * v2);
+  U[6] = rho * (T22 + v2 * v2);
+  U[7] = q1 + E * v1 + rho * (T11 * v1 + T12 * v2);
+  U[8] = q2 + E * v2 + rho * (T12 * v1 + T22 * v2);
+}
+
+// Conservative (src/Flux.c:61-74 with src/primDef.h:9-20)
+__device__ __forceinline__ void conservative(const double (&P)[NV], double (&U)[NV]) {
+  const double vs = P[1] * P[1] + P[2] * P[2];
+  const double E = 0.5 * P[0] * vs + 1.5 * P[0] * P[3];
+  moments_e(P[0], P[1], P[2], E, P[4], P[5], P[6], P[7], P[8], U);
+}
+
+// Grad-13 flux along x of a moment vector (src/Flux.c:79-119)
+__device__ __forceinline__ void grad13_flux_x(const double (&U)[NV], double (&F)[NV]) {
+  const double rho = U[0];
+  const double v1 = U[1] / rho, v2 = U[2] / rho;
+  const double vs = v1 * v1 + v2 * v2;
+  const double th = (2 * U[3] / rho - vs) / 3;
+  const double E = U[3];
+  const double T11 = U[4] / rho - v1 * v1;
+  const double T12 = U[5] / rho - v1 * v2;
+  const double T22 = U[6] / rho - v2 * v2;
+  const double q1 = U[7] - E * v1 - rho * (T11 * v1 + T12 * v2);
+  const double q2 = U[8] - E * v2 - rho * (T12 * v1 + T22 * v2);
+  const double M111 = 1.2 * q1 / rho;
+  const double M121 = 0.4 * q2 / rho, M112 = M121;
+  const double M221 = 0.4 * q1 / rho, M122 = M221;
+  const double R11 = 5 * th * th + 7 * th * (T11 - th);
+  const double R12 = 7 * th * T12;
+  F[0] = rho * v1;
+  F[1] = rho * (T11 + v1 * v1);
+  F[2] = rho * (T12 + v1 * v2);
+  F[3] = E * v1 + rho * (T11 * v1 + T12 * v2) + q1;
+  F[4] = rho * (M111 + 3 * T11 * v1 + v1 * v1 * v1);
+  F[5] = rho * (M121 + T11 * v2 + 2 * T12 * v1 + v1 * v2 * v1);
+  F[6] = rho * (M221 + T22 * v1 + 2 * T12 * v2 + v2 * v2 * v1);
+  F[7] = 2 * (q1 + rho * (T11 * v1 + T12 * v2)) * v1 + E * v1 * v1 +
+         rho * (M111 * v1 + M112 * v2) + 0.5 * rho * (T11 * vs + R11);
+  F[8] = q2 * v1 + q1 * v2 + rho * (v1 * v2 * (T11 + T22) + 1.5 * T12 * vs) + E * v1 * v2 +
+         rho * (M121 * v1 + M122 * v2) + 0.5 * rho * R12;
+}
+
+// flux through a face of unit normal (nx, ny): rotate, x-flux, rotate back
+// (src/Flux.c:126-172).  The products with 0 and +-1 are kept: they fix the
+// signs of zeros exactly as the reference computes them.
+__device__ __forceinline__ void flux_normal(const double (&U)[NV], double (&F)[NV], double nx,
+                                            double ny) {
+  const double tx = ny, ty = -nx;
+  double W[NV], G[NV], a, b;
+  W[0] = U[0];
+  W[1] = U[1] * nx + U[2] * ny;
+  W[2] = U[1] * tx + U[2] * ty;
+  W[3] = U[3];
+  a = U[4] * nx + U[5] * ny;
+  b = U[5] * nx + U[6] * ny;
+  W[4] = a * nx + b * ny;
+  W[5] = a * tx + b * ty;
+  a = U[4] * tx + U[5] * ty;
+  b = U[5] * tx + U[6] * ty;
+  W[6] = a * tx + b * ty;
+  W[7] = U[7] * nx + U[8] * ny;
+  W[8] = U[7] * tx + U[8] * ty;
+  grad13_flux_x(W, G);
+  F[0] = G[0];
+  F[1] = G[1] * nx + G[2] * tx;
+  F[2] = G[1] * ny + G[2] * ty;
+  F[3] = G[3];
+  a = G[4] * nx + G[5] * tx;
+  b = G[5] * nx + G[6] * tx;
+  F[4] = a * nx + b * tx;
+  F[5] = a * ny + b * ty;
+  a = G[4] * ny + G[5] * ty;
+  b = G[5] * ny + G[6] * ty;
+  F[6] = a * ny + b * ty;
+  F[7] = G[7] * nx + G[8] * tx;
+  F[8] = G[7] * ny + G[8] * ty;
+}
+
+// damping factor of the direct production integration (src/Flux.c:213-223)
+template <int FLAG>
+__device__ __forceinline__ double rdamp(double z) {
+  if (FLAG == -1 || FLAG == 0) return (1 + 0.5 * z - 0.25 * z * z) / (1 + z + 0.25 * z * z);
+  if (FLAG == 1) return (1 + z) / (1 + z + 0.25 * z * z);
+  if (FLAG == 2) return (1 + 0.5 * z) / (1 + 0.5 * z);
+  return 1.0 / (1 + 0.5 * z);
+}
+
+// ProductionsDirect (src/Flux.c:230-267) with CollFreq and ExternalForce
+// (src/Scenario.c:28-42; nu0 = 1, force (F, 0)), starting from the primitives P
+// of the input moments.  Writes the relaxed moments, returns 0.5*(1 - R(2z/3)).
+template <int FLAG>
+__device__ __forceinline__ double relax(const double (&P)[NV], double (&Out)[NV], double dt,
+                                        double Kn, double F) {
+  const double rho = P[0], th = P[3];
+  double v1 = P[1], v2 = P[2];
+  double vs = v1 * v1 + v2 * v2;
+  double E = 0.5 * rho * vs + 1.5 * rho * th;
+  const double nu0 = 1.0;
+  const double coll = (nu0 * rho * sqrt(th) / Kn) * dt;
+  if (FLAG == 0 || FLAG == 2) {
+    const double g0 = F, g1 = 0.0;
+    v1 += dt * g0;
+    v2 += dt * g1;
+    vs = v1 * v1 + v2 * v2;
+    E = 0.5 * rho * vs + 1.5 * rho * th;
+  }
+  const double d1 = rdamp<FLAG>(coll);
+  const double d2 = rdamp<FLAG>(2.0 / 3 * coll);
+  const double T11 = d1 * (P[4] - th) + th;
+  const double T12 = d1 * P[5];
+  const double T22 = d1 * (P[6] - th) + th;
+  moments_e(rho, v1, v2, E, T11, T12, T22, d2 * P[7], d2 * P[8], Out);
+  return 0.5 * (1 - d2);
+}
+
+// only the CFL share of relax<FLAG> (same z, same factor)
+template <int FLAG>
+__device__ __forceinline__ double relax_cfl(const double (&P)[NV], double dt, double Kn) {
+  const double nu0 = 1.0;
+  const double coll = (nu0 * P[0] * sqrt(P[3]) / Kn) * dt;
+  return 0.5 * (1 - rdamp<FLAG>(2.0 / 3 * coll));
+}
+
+// Limit1 (src/Limiter.c:26-59)
+__device__ __forceinline__ double superbee_phi(double r) {
+  if (r < 0.0) return 0.0;
+  if (r < 0.5) return 2 * r;
+  if (r < 1.0) return 1.0;
+  if (r < 2.0) return r;
+  return 2.0;
+}
+
+template <int LIM>
+__device__ __forceinline__ double limit(double d1, double d2) {
+  if (LIM == 0) return 0.0;
+  if (LIM == 1) return 0.5 * (d1 + d2);
+  if (LIM == 2) return 0.5 * (rsgn(d1) + rsgn(d2)) * rmin(fabs(d1), fabs(d2));
+  if (LIM == 3) return d1 * superbee_phi(d2 / d1);
+  const double eps = 1.0e-10;
+  const double w1 = fabs(d1) + eps, w2 = fabs(d2) + eps;
+  return (w1 * d2 + w2 * d1) / (w1 + w2);
+}
+
+// FnumHLLE (src/Flux.c:308-379) for a face with left/right primitives.
+// DIR = 1: x face (normal (1,0)), DIR = 2: y face (normal (0,1)).  The
+// diffusive scale FFlux/GFlux return is 0, so lamDiff(0/(cMax*dx)) is 1 for
+// every cMax and cMax/1.0 == cMax: the division is omitted without changing a bit.
+template <int DIR>
+__device__ __forceinline__ double hll(const double (&PL)[NV], const double (&PR)[NV],
+                                      double (&flx)[NV]) {
+  constexpr double nx = DIR == 1 ? 1.0 : 0.0, ny = DIR == 1 ? 0.0 : 1.0;
+  const double cR = 2.0 * sqrt(5.0 / 3 * PR[3]);
+  const double cL = 2.0 * sqrt(5.0 / 3 * PL[3]);
+  double UL[NV], UR[NV], fL[NV], fR[NV];
+  conservative(PL, UL);
+  flux_normal(UL, fL, nx, ny);
+  conservative(PR, UR);
+  flux_normal(UR, fR, nx, ny);
+  const double vR = PR[DIR], vL = PL[DIR];
+  const double cMax = fabs(0.5 * (vL + vR)) + rmax(cR, cL);
+  const double lamL = rmin(vL - cL, 0.0);
+  const double lamR = rmax(vR + cR, 0.0);
+  const double alph = lamR - lamL;
+  if (alph > 0.0) {
+#pragma unroll
+    for (int n = 0; n < NV; n++)
+      flx[n] = (lamR * fL[n] - lamL * fR[n] + lamL * lamR * (UR[n] - UL[n])) / alph;
+  } else {
+#pragma unroll
+    for (int n = 0; n < NV; n++) flx[n] = 0.5 * (fL[n] + fR[n]);
+  }
+  return cMax;
+}
+
+}  // namespace mbm

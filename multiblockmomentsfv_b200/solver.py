@@ -1,0 +1,191 @@
+"""Python front end of the device solver: the reference's host loop (main(),
+src/Main.c:61-164) over the C ABI.
+
+    deck = blockfile.parse_file("cases/squareSmall.txt")
+    with Solver(deck, Scenario.named("riemann2d")) as s:
+        s.initialise()
+        t, n, rej = s.steps(0.0, 0.05)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+from . import blockfile as bf
+from . import output as out
+from . import scenario as sc
+
+L_DATA, L_TMP, L_NEW = _abi.L_DATA, _abi.L_TMP, _abi.L_NEW
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Solver:
+    """Device state of one deck: three layers per block on one GPU."""
+
+    def __init__(self, deck: bf.Deck, scenario: Optional[sc.Scenario] = None, device: int = 0,
+                 show_every: int = 20, stream: Optional[int] = None, segment_rows: int = 0,
+                 max_attempts: int = 0):
+        self.deck = deck
+        self.scenario = scenario
+        self.L = _abi.lib()
+        self._descs = _abi.block_descs(deck.blocks)
+        p = _abi.Params()
+        p.Kn, p.F, p.limiter, p.mode = deck.Kn, deck.F, deck.limiter, _abi.MODE_EXACT
+        p.device, p.show_every, p.max_attempts, p.segment_rows = device, show_every, max_attempts, segment_rows
+        p.stream = stream
+        self._params = p
+        ctx = C.c_void_p()
+        st = self.L.mbm_create(self._descs, len(deck.blocks), C.byref(p), C.byref(ctx))
+        if st != _abi.MBM_OK:
+            raise _abi.MBMError(st, self.L.mbm_last_error(None).decode())
+        self.ctx = ctx
+        if scenario is not None:
+            self.set_dirichlet_from(scenario, 0.0)
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.L.mbm_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int) -> None:
+        _abi.check(st, self.ctx)
+
+    # -- data -----------------------------------------------------------------
+    def upload(self, layer: int, b: int, U: np.ndarray) -> None:
+        blk = self.deck.blocks[b]
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if U.size != blk.cells * bf.NV:
+            raise ValueError("layer array has the wrong size")
+        self._check(self.L.mbm_upload(self.ctx, layer, b, _dptr(U)))
+
+    def download(self, layer: int, b: int, out_arr: Optional[np.ndarray] = None) -> np.ndarray:
+        blk = self.deck.blocks[b]
+        U = out_arr if out_arr is not None else np.empty((blk.nyp, blk.nxp, bf.NV))
+        self._check(self.L.mbm_download(self.ctx, layer, b, _dptr(U)))
+        return U
+
+    def layers(self, layer: int = L_DATA) -> List[np.ndarray]:
+        return [self.download(layer, b) for b in range(len(self.deck.blocks))]
+
+    def set_dirichlet(self, b: int, side: int, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self._check(self.L.mbm_set_dirichlet(self.ctx, b, side, _dptr(v)))
+
+    def set_dirichlet_from(self, s: sc.Scenario, t: float = 0.0) -> None:
+        for b, blk in enumerate(self.deck.blocks):
+            for side in range(4):
+                if blk.bc[side] <= -2:
+                    self.set_dirichlet(b, side, sc.dirichlet_edge(s, blk, side, t))
+
+    def initialise(self) -> None:
+        """Interior from the scenario, ghosts by SetBoundary (src/Main.c:113-138)."""
+        if self.scenario is None:
+            raise ValueError("no scenario given")
+        for b, blk in enumerate(self.deck.blocks):
+            self.upload(L_DATA, b, sc.initial_block(self.scenario, blk))
+        self.set_boundary(L_DATA, 0.0)
+
+    # -- the path ---------------------------------------------------------------
+    def set_boundary(self, layer: int, t: float) -> None:
+        self._check(self.L.mbm_set_boundary(self.ctx, layer, t))
+
+    def update(self, out_layer: int, in_layer: int, data0_layer: int, dt: float, t: float,
+               heun: int) -> np.ndarray:
+        cfl = np.zeros(len(self.deck.blocks))
+        self._check(self.L.mbm_update(self.ctx, out_layer, in_layer, data0_layer, dt, t, heun, _dptr(cfl)))
+        return cfl
+
+    def time_update(self, dt: float, t: float) -> float:
+        v = C.c_double(0.0)
+        self._check(self.L.mbm_time_update(self.ctx, dt, t, C.byref(v)))
+        return v.value
+
+    def steps(self, t: float, tend: float, CFLmax: float = 1.0, CFLreg: Optional[float] = None,
+              max_steps: int = 0):
+        """Steps(): returns (t, accepted steps, rejected attempts).  max_steps > 0
+        also ends the loop after that many accepted steps."""
+        CFLreg = self.deck.CFL if CFLreg is None else CFLreg
+        tt = C.c_double(t)
+        n = C.c_int(0)
+        r = C.c_int(0)
+        self._check(self.L.mbm_steps_capped(self.ctx, C.byref(tt), tend, CFLmax, CFLreg, max_steps,
+                                            C.byref(n), C.byref(r)))
+        return tt.value, n.value, r.value
+
+    def attempts(self) -> int:
+        a = C.c_int(0)
+        self._check(self.L.mbm_attempts(self.ctx, C.byref(a)))
+        return a.value
+
+    def time_stage(self, heun: int, dt: float, reps: int = 10) -> float:
+        """Mean device milliseconds of one stage-kernel launch (CUDA events)."""
+        ms = C.c_double(0.0)
+        self._check(self.L.mbm_time_stage(self.ctx, heun, dt, reps, C.byref(ms)))
+        return ms.value
+
+    def trace(self) -> np.ndarray:
+        cap = 4096
+        buf = np.zeros((cap, 4))
+        n = C.c_int(0)
+        self._check(self.L.mbm_trace(self.ctx, _dptr(buf), cap, C.byref(n)))
+        return buf[:n.value].copy()
+
+
+def ghost_map(blocks: Sequence[bf.Block]) -> np.ndarray:
+    """Resolved ghost sources (host only, no GPU): rows {dst_block, dst_cell, src,
+    src_block | flags << 16}."""
+    L = _abi.lib()
+    descs = _abi.block_descs(blocks)
+    n = C.c_int(0)
+    _abi.check(L.mbm_ghost_map(descs, len(blocks), None, 0, C.byref(n)))
+    arr = np.zeros((max(1, n.value), 4), dtype=np.int32)
+    _abi.check(L.mbm_ghost_map(descs, len(blocks), arr.ctypes.data_as(C.POINTER(C.c_int)), n.value,
+                               C.byref(n)))
+    return arr[:n.value]
+
+
+def run(deck: bf.Deck, scenario: sc.Scenario, out_dir: str, single: bool = True, device: int = 0,
+        verbose: bool = True, show_every: int = 20):
+    """The reference's main() loop on the device: initial state and output at t=0,
+    then Steps + Output per output time (src/Main.c:138-156).  Returns (writer, steps)."""
+    w = out.Writer(out_dir, deck, scenario.type_name, single)
+    with Solver(deck, scenario, device=device, show_every=show_every) as s:
+        s.initialise()
+        w.write(s.layers(), 0.0, -1)
+        t, nmax = 0.0, 0
+        cells = deck.full_grid_size
+        for tn in deck.t_out:
+            t0 = time.perf_counter()
+            t, n, rej = s.steps(t, tn, 1.0, deck.CFL)
+            el = time.perf_counter() - t0
+            if verbose:
+                for step, cfl, tt, dt in s.trace():
+                    print(" step: %3d... done.  CFL: %lf, time: %lf, next dt: %lf" % (step, cfl, tt, dt))
+                perf = el * 1e6 / max(1, cells * (n + rej))
+                print("   %d steps (%d rejected) to t = %g in %.3f s, %.4f us per cell-update" %
+                      (n, rej, t, el, perf))
+            nmax += n
+            w.write(s.layers(), t, nmax)
+    if verbose:
+        print("\n Done after %d steps.\n" % nmax)
+    return w, nmax

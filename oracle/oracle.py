@@ -217,3 +217,98 @@ def run_reference(deck_path: str, out_dir: str, scenario: sc.Scenario, extra=(),
     os.makedirs(out_dir, exist_ok=True)
     return subprocess.run([exe, "-bfile", deck_path, "-out", out_dir, *extra], env=env,
                           capture_output=True, text=True, check=True)
+
+
+# ------------------------------------------------------------------------------
+# the reference itself (oracle/_ref/libmbmref.so: the reference's sources, main renamed)
+class _DBPoint(C.Structure):
+    _fields_ = [("i", C.c_int), ("j", C.c_int)]
+
+
+class _DBRange(C.Structure):
+    _fields_ = [("level", C.c_uint), ("lfb", _DBPoint), ("rbt", _DBPoint)]
+
+
+class DBBlock(C.Structure):
+    """DB_Block of src/defs.h:59-68."""
+    _fields_ = [("layer", C.c_void_p * 3), ("Aux", C.c_void_p), ("block_id", C.c_int),
+                ("range", _DBRange), ("x", C.c_double), ("y", C.c_double), ("z", C.c_double),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+                ("boundary", C.c_int * 4)]
+
+
+_ref = None
+
+
+def ref_lib():
+    """Load oracle/_ref/libmbmref.so (None when the reference was not built here)."""
+    global _ref
+    if _ref is None:
+        p = os.path.join(REF_DIR, "libmbmref.so")
+        if not os.path.exists(p):
+            return None
+        L = C.CDLL(p)
+        P = C.POINTER
+        L.Update.restype = C.c_double
+        L.Update.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, DBBlock, C.c_void_p,
+                             C.c_double, C.c_double, C.c_int]
+        L.TimeUpdate.restype = C.c_double
+        L.TimeUpdate.argtypes = [P(DBBlock), C.c_int, C.c_double, C.c_double]
+        L.SetBoundary.argtypes = [P(DBBlock), C.c_int, C.c_int, C.c_double]
+        L.Steps.restype = C.c_int
+        L.Steps.argtypes = [P(DBBlock), C.c_int, P(C.c_double), C.c_double, C.c_double, C.c_double]
+        _ref = L
+    return _ref
+
+
+class Reference:
+    """The reference's own Update / TimeUpdate / SetBoundary / Steps on numpy layers."""
+
+    def __init__(self, deck: bf.Deck):
+        self.L = ref_lib()
+        if self.L is None:
+            raise FileNotFoundError("oracle/_ref/libmbmref.so not built")
+        self.deck = deck
+        nb = len(deck.blocks)
+        self.B = (DBBlock * nb)()
+        self.layer = [[None] * nb for _ in range(3)]
+        self.aux = []
+        for k, b in enumerate(deck.blocks):
+            for l in range(3):
+                self.layer[l][k] = np.zeros((b.nyp, b.nxp, NV))
+                self.B[k].layer[l] = self.layer[l][k].ctypes.data
+            self.aux.append(np.zeros((b.nyp, b.nxp, 3 * NV)))
+            self.B[k].Aux = self.aux[k].ctypes.data
+            self.B[k].block_id = b.block_id
+            self.B[k].range.level = 0
+            self.B[k].range.lfb.i = self.B[k].range.lfb.j = 1
+            self.B[k].range.rbt.i = b.nxp
+            self.B[k].range.rbt.j = b.nyp
+            self.B[k].x, self.B[k].y, self.B[k].z = b.x0, b.y0, 0.0
+            self.B[k].dx, self.B[k].dy, self.B[k].dz = b.dx, b.dy, 1.0
+            for s in range(4):
+                self.B[k].boundary[s] = b.bc[s]
+        self.set_params(deck)
+
+    def set_params(self, deck: bf.Deck):
+        C.c_double.in_dll(self.L, "Kn").value = deck.Kn
+        C.c_double.in_dll(self.L, "F").value = deck.F
+        C.c_double.in_dll(self.L, "R13").value = deck.R13
+        C.c_int.in_dll(self.L, "Limiter").value = deck.limiter
+
+    def set_layer(self, l: int, b: int, U: np.ndarray):
+        self.layer[l][b][...] = U.reshape(self.layer[l][b].shape)
+
+    def get_layer(self, l: int, b: int) -> np.ndarray:
+        return self.layer[l][b].copy()
+
+    def update(self, b, out_l, in_l, d0_l, dt, t, heun) -> float:
+        return self.L.Update(self.layer[out_l][b].ctypes.data, self.layer[in_l][b].ctypes.data,
+                             self.aux[b].ctypes.data, self.B[b], self.layer[d0_l][b].ctypes.data,
+                             dt, t, heun)
+
+    def set_boundary(self, l: int, t: float):
+        self.L.SetBoundary(self.B, len(self.deck.blocks), l, t)
+
+    def time_update(self, dt: float, t: float) -> float:
+        return self.L.TimeUpdate(self.B, len(self.deck.blocks), dt, t)

@@ -1,0 +1,125 @@
+"""Host logic without a GPU: the C-ABI library loads and exports its symbols, the
+resolved ghost map equals the reference's two-sweep SetBoundary, the deck parser
+and the output writer."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import helpers as H
+from multiblockmomentsfv_b200 import _abi, blockfile as bf, output as out, scenario as sc, solver
+
+
+def test_library_loads_and_exports_every_header_symbol():
+    L = _abi.lib()
+    header = open(os.path.join(H.HERE, "..", "include", "mbm_b200.h")).read()
+    declared = set(re.findall(r"\b(mbm_[a-z_]+)\s*\(", header))
+    assert declared == set(_abi.EXPORTS)
+    for name in declared:
+        assert hasattr(L, name), name
+    assert L.mbm_version() == 1
+    assert L.mbm_strerror(_abi.MBM_EINVAL) == b"invalid argument"
+
+
+def test_create_without_device_fails_loudly():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(_abi.MBMError) as e:
+        solver.Solver(H.deck("squareSmall"))
+    assert e.value.status == _abi.MBM_ENODEV
+
+
+@pytest.mark.parametrize("name", ["squareSmall", "square4", "square4Box", "Lshape", "ffs", "ffs28",
+                                  "square16Uniform"])
+def test_ghost_map_equals_two_sweep_fill(oracle_mod, name):
+    """The gather map reproduces SetBoundary bit for bit on the reference decks
+    (open, wall, Dirichlet and sync edges, convex and re-entrant corners)."""
+    d = H.deck(name)
+    if name in ("square4", "Lshape", "square16Uniform", "square4Box"):
+        d.blocks = [bf.Block(b.block_id, b.xmin, b.xmax, b.ymin, b.ymax, max(3, b.nx // 10),
+                             max(3, b.ny // 10), b.bc) for b in d.blocks]
+    _check_map(oracle_mod, d, np.random.default_rng(1))
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_ghost_map_random_layouts(oracle_mod, seed):
+    rng = np.random.default_rng(100 + seed)
+    _check_map(oracle_mod, H.random_deck(rng, max_n=7), rng)
+
+
+def _check_map(oracle_mod, d, rng):
+    scn = sc.Scenario.named("ffs")
+    orc = oracle_mod.Oracle(d, scn)
+    layers = []
+    for b, blk in enumerate(d.blocks):
+        U = rng.standard_normal((blk.nyp, blk.nxp, bf.NV))
+        orc.set_layer(1, b, U)
+        layers.append(U.copy())
+    orc.set_boundary(1, 0.0)
+    entries = solver.ghost_map(d.blocks)
+    rows = []
+    for b, blk in enumerate(d.blocks):
+        for side in range(4):
+            if blk.bc[side] <= -2:
+                rows.append(sc.dirichlet_edge(scn, blk, side).reshape(-1, bf.NV))
+    dirichlet = np.concatenate(rows) if rows else None
+    H.apply_ghost_map(entries, layers, dirichlet)
+    for b in range(len(d.blocks)):
+        H.assert_bitwise(layers[b], orc.get_layer(1, b), f"block {b + 1}")
+
+
+def test_ghost_map_rejects_bad_tables():
+    B = bf.Block
+    with pytest.raises(_abi.MBMError):      # partner does not exist
+        solver.ghost_map([B(1, 0, 1, 0, 1, 5, 5, (0, 2, 0, 0))])
+    with pytest.raises(_abi.MBMError):      # non-conforming interface
+        solver.ghost_map([B(1, 0, 1, 0, 1, 5, 5, (0, 2, 0, 0)), B(2, 1, 2, 0, 1, 5, 6, (1, 0, 0, 0))])
+    with pytest.raises(_abi.MBMError):      # too narrow: a ghost cell keeps no defined source
+        solver.ghost_map([B(1, 0, 1, 0, 1, 1, 5, (-1, -1, 0, 0))])
+
+
+def test_dirichlet_edge_order():
+    blk = bf.Block(1, -1.0, 0.0, -1.0, 1.0, 4, 5, (-2, 0, 0, 0))
+    v = sc.dirichlet_edge(sc.Scenario.named("riemann2d"), blk, 0)
+    assert v.shape == (blk.nyp, 3, bf.NV)
+    x, y = blk.centres()
+    ref = sc.initial_state(sc.Scenario.named("riemann2d"), x[4, 3 - 2], y[4, 3 - 2])
+    assert np.array_equal(v[4, 1], ref)
+
+
+def test_deck_parser_reads_every_reference_deck():
+    for f in sorted(os.listdir(H.DECKS)):
+        d = bf.parse_file(os.path.join(H.DECKS, f))
+        assert d.blocks and d.t_out
+    d = H.deck("squareSmall")
+    assert (d.Kn, d.CFL, d.limiter, d.full_grid_size) == (0.001, 0.95, bf.LIM_HARMONIC, 400)
+    assert d.t_out == [0.05, 0.1, 0.15000000000000002, 0.2, 0.25, 0.30000000000000004]
+    assert d.blocks[0].x0 == -1.25
+    d2 = d.with_cli(Kn="0.01")
+    assert d2.Kn == float(np.float32(0.01)) != 0.01
+    rt = bf.parse_text(bf.format_deck(H.deck("ffs28")))
+    assert rt.blocks == H.deck("ffs28").blocks
+
+
+def test_convert_names():
+    assert out.convert(0.05) == "0p05"
+    assert out.convert(0.001) == "0p001"
+    assert out.convert(0.3) == "0p3"
+    assert out.convert(1.0) == "1p0"
+
+
+def test_scenario_matches_oracle_state(oracle_mod):
+    s = sc.Scenario.seeded_quadrant(3)
+    xs = np.linspace(-1, 1, 7)
+    for x in xs:
+        for y in xs:
+            U = np.zeros(9)
+            oracle_mod.lib().orc_initial_state(C.byref(oracle_mod.c_scenario(s)), x, y, 0.0,
+                                               U.ctypes.data_as(C.POINTER(C.c_double)))
+            assert np.array_equal(U, sc.initial_state(s, x, y))

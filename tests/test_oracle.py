@@ -1,0 +1,123 @@
+"""The oracle pinned: the C restatement against the reference goldens (committed
+fixtures) and, where the reference sources were built here, against the
+reference's own functions on seeded random states."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import helpers as H
+from multiblockmomentsfv_b200 import output as out
+from multiblockmomentsfv_b200 import scenario as sc
+
+
+def golden_values(name):
+    z = np.load(os.path.join(H.GOLDEN, name))
+    return z
+
+
+def test_squareSmall_golden_bitwise(oracle_mod, tmp_path):
+    """All 7 output levels of reference/squareSmall.ref, Float32, bit for bit (112 steps)."""
+    d = H.deck("squareSmall")
+    w, n = oracle_mod.run_deck(d, sc.Scenario.named("riemann2d"), str(tmp_path))
+    assert n == 112
+    zones, prec = out.read(w.hdr)
+    g = golden_values("squareSmall_ref.npz")
+    mine = np.concatenate([z["values"].astype(np.float32).ravel() for z in zones])
+    assert prec == "Float32"
+    assert [z["block"] for z in zones] == list(g["block"])
+    assert [z["strand"] for z in zones] == list(g["strand"])
+    assert np.array_equal(mine.view(np.uint32), g["values"].view(np.uint32))
+
+
+@pytest.mark.slow
+def test_square4_golden_bitwise(oracle_mod, tmp_path):
+    """reference/square4.ref at t = 0.3 bit for bit; 352 steps; the progress trace
+    matches the golden console log to its printed precision."""
+    d = H.deck("square4")
+    o = oracle_mod.Oracle(d, sc.Scenario.named("riemann2d"))
+    o.initialise()
+    t, total, traces = 0.0, 0, []
+    for tn in d.t_out:
+        t, n, rej, tr = o.steps(t, tn)
+        total += n
+        traces.append(tr)
+    ref = json.load(open(os.path.join(H.GOLDEN, "square4_ref_trace.json")))
+    assert total == ref["total_steps"] == 352
+    recs = [(k, int(r[0]), r[1], r[2], r[3]) for k, tr in enumerate(traces) for r in tr]
+    assert len(recs) == len(ref["records"])
+    for a, b in zip(recs, ref["records"]):
+        assert a[0] == b[0] and a[1] == b[1]
+        assert ["%f" % v for v in a[2:]] == ["%f" % v for v in b[2:]]
+    g = golden_values("square4_ref_t0p3.npz")
+    vals = np.concatenate([out.physical_fields(U[2:-2, 2:-2]).transpose(1, 0, 2).astype(np.float32).ravel()
+                           for U in o.layers()])
+    assert np.array_equal(vals.view(np.uint32), g["values"].view(np.uint32))
+
+
+def test_oracle_output_writer_matches_manifest(oracle_mod, tmp_path):
+    d = H.deck("squareSmall", t_out=[0.05])
+    w, n = oracle_mod.run_deck(d, sc.Scenario.named("riemann2d"), str(tmp_path))
+    text = open(w.hdr).read()
+    assert "solver = Grad13Riemann2D" in text and "FullGridSize = 400" in text
+    assert os.path.basename(w.hdr) == "Grad13Riemann2D_nst400_Kn0p001_tAll.hdr"
+    zones, _ = out.read(w.hdr)
+    assert [z["strand"] for z in zones] == [1, 1, 1, 1, n + 1, n + 1, n + 1, n + 1]
+
+
+needs_ref = pytest.mark.skipif(not os.path.exists(os.path.join(H.HERE, "..", "oracle", "_ref", "libmbmref.so")),
+                               reason="reference sources not built here")
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", range(6))
+def test_oracle_equals_reference_update(oracle_mod, seed):
+    """Update() and SetBoundary() of the reference versus the restatement on random
+    admissible states, every limiter, both Heun flags, bitwise incl. the CFL."""
+    rng = np.random.default_rng(seed)
+    d = H.random_deck(rng)
+    d.limiter = seed % 5
+    d.F = 0.3 if seed % 2 else 0.0
+    ref = oracle_mod.Reference(d)
+    orc = oracle_mod.Oracle(d, sc.Scenario.named("riemann2d"))
+    dt = 0.002
+    for b, blk in enumerate(d.blocks):
+        for l in range(3):
+            U = H.random_layer(rng, blk)
+            ref.set_layer(l, b, U)
+            orc.set_layer(l, b, U)
+    for heun, (o_l, i_l, d0_l) in ((0, (1, 0, 0)), (1, (2, 1, 0))):
+        for b in range(len(d.blocks)):
+            c1 = ref.update(b, o_l, i_l, d0_l, dt, 0.1, heun)
+            c2 = orc.update(b, o_l, i_l, d0_l, dt, 0.1, heun)
+            assert np.float64(c1).view(np.uint64) == np.float64(c2).view(np.uint64)
+            H.assert_bitwise(orc.get_layer(o_l, b), ref.get_layer(o_l, b), f"update b{b} heun{heun}")
+    ref.set_boundary(2, 0.1)
+    orc.set_boundary(2, 0.1)
+    for b in range(len(d.blocks)):
+        H.assert_bitwise(orc.get_layer(2, b), ref.get_layer(2, b), f"boundary b{b}")
+
+
+@needs_ref
+def test_oracle_equals_reference_time_update(oracle_mod):
+    rng = np.random.default_rng(11)
+    d = H.deck("Lshape")
+    d.blocks = [type(b)(b.block_id, b.xmin, b.xmax, b.ymin, b.ymax, b.nx // 10, b.ny // 10, b.bc)
+                for b in d.blocks]
+    ref = oracle_mod.Reference(d)
+    orc = oracle_mod.Oracle(d, sc.Scenario.named("riemann2d"))
+    for b, blk in enumerate(d.blocks):
+        U = H.random_layer(rng, blk)
+        ref.set_layer(0, b, U)
+        orc.set_layer(0, b, U)
+    ref.set_boundary(0, 0.0)
+    orc.set_boundary(0, 0.0)
+    for k in range(3):
+        c1 = ref.time_update(0.001, 0.001 * k)
+        c2 = orc.time_update(0.001, 0.001 * k)
+        assert c1 == c2
+        for b in range(len(d.blocks)):
+            H.assert_bitwise(orc.get_layer(2, b), ref.get_layer(2, b), f"time_update b{b}")
+            ref.set_layer(0, b, ref.get_layer(2, b))
+            orc.set_layer(0, b, orc.get_layer(2, b))
