@@ -1,0 +1,59 @@
+"""Drop-in: the reference's own C host (main, block-file parser, Mesh, Output),
+linked with the GPU Steps of multiblockmomentsfv_b200/shim/mbm_steps_shim.c
+(oracle/_ref/moments_b200), against the unmodified reference build
+(oracle/_ref/moments) on the same decks.  Both write Float64 output (-double);
+the result files must agree exactly (abstol = reltol = 0)."""
+import os
+import subprocess
+
+import pytest
+
+import helpers as H
+from multiblockmomentsfv_b200 import output as out
+
+REF = os.path.join(H.HERE, "..", "oracle", "_ref")
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not os.path.exists(os.path.join(REF, "moments_b200")),
+                                 reason="drop-in binary not built (make -C oracle b200)")]
+
+
+def _run(exe, deck, out_dir, scenario, extra=()):
+    env = dict(os.environ, MBM_SCENARIO=scenario, OMP_NUM_THREADS="1")
+    r = subprocess.run([os.path.join(REF, exe), "-bfile", deck, "-out", out_dir, "-double", *extra],
+                       env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    hdrs = [f for f in os.listdir(out_dir) if f.endswith(".hdr")]
+    assert len(hdrs) == 1
+    return os.path.join(out_dir, hdrs[0]), r.stdout
+
+
+def _deck(tmp_path, name, t_list=None, dt_out=None):
+    text = open(os.path.join(H.DECKS, name + ".txt")).read()
+    lines = []
+    for line in text.splitlines():
+        s = line.strip()
+        if t_list is not None and s.startswith("t_list"):
+            line = f"t_list = {t_list}"
+        if dt_out is not None and s.startswith("dt_out"):
+            line = f"dt_out = {dt_out}"
+        lines.append(line)
+    p = tmp_path / (name + ".txt")
+    p.write_text("\n".join(lines) + "\n")
+    return str(p)
+
+
+@pytest.mark.parametrize("name,scenario,t_list,dt_out,extra", [
+    ("squareSmall", "riemann2d", None, None, ()),
+    ("square4", "riemann2d", "0.1", "0.05", ("-limiter", "superbee")),
+    ("Lshape", "riemann2d", "0.02", "0.01", ("-Kn", "0.005")),
+    ("ffs28", "ffs", "0.02", "0", ()),
+    ("square4Box", "riemann2d", "0.05", "0", ("-R13", "1")),
+])
+def test_reference_host_with_gpu_steps(tmp_path, name, scenario, t_list, dt_out, extra):
+    deck = _deck(tmp_path, name, t_list, dt_out)
+    a, log_gpu = _run("moments_b200", deck, str(tmp_path / "gpu"), scenario, extra)
+    b, _ = _run("moments", deck, str(tmp_path / "ref"), scenario, extra)
+    assert os.path.basename(a) == os.path.basename(b)
+    ok, mx, msg = out.compare(a, b, 0.0, 0.0)
+    assert ok and mx == 0.0, msg
+    assert "(gpu)" in log_gpu or "Done after" in log_gpu
