@@ -53,7 +53,8 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   const CaseDev& cs = a.cases[B.case_id];
   if (cs.done) return;
   const int cur = cs.cur;
-  const double dt = cs.dt, Kn = cs.Kn, Fx = cs.F;
+  const double dt = cs.dt, Fx = cs.F;
+  const Recip Kn(cs.Kn);
   const double* __restrict__ in = a.buf[phys_layer(a.sel_in, cur)] + B.off;
   const double* __restrict__ d0 = a.buf[phys_layer(a.sel_d0, cur)] + B.off;
   double* __restrict__ out = a.buf[phys_layer(a.sel_out, cur)] + B.off;
@@ -67,6 +68,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   const bool col_out = lane >= 2 && lane <= 29 && C >= NG && C <= nxp - 1 - NG;
   const double dx = B.dx, dy = B.dy;
   const double dtdx = dt / dx, dtdy = dt / dy;
+  const Recip rdx(dx), rdy(dy);
   const double hdx = 0.5 * dx, hdy = 0.5 * dy;
   double lamx = 0.0, lamy = 0.0, prod = 0.0;
 
@@ -92,9 +94,9 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   };
   // y slope from three consecutive rows (src/Main.c:348-349)
   auto slope = [&](const double (&Pm)[NV], const double (&P0)[NV], const double (&Pp)[NV],
-                   double h, double (&S)[NV]) {
+                   const Recip& h, double (&S)[NV]) {
 #pragma unroll
-    for (int n = 0; n < NV; n++) S[n] = limit<LIM>(P0[n] - Pm[n], Pp[n] - P0[n]) / h;
+    for (int n = 0; n < NV; n++) S[n] = h.div(limit<LIM>(P0[n] - Pm[n], Pp[n] - P0[n]));
   };
   // y face between rows J and J+1 (src/Main.c:359-365)
   auto yface = [&](const double (&Pb)[NV], const double (&Sb)[NV], const double (&Pt)[NV],
@@ -119,14 +121,14 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
       prim_at(J0 - 1, Pm);
       prim_at(J0, P0);
       prim_at(J0 + 1, P1);
-      slope(Pmm, Pm, P0, dy, Sm);
-      slope(Pm, P0, P1, dy, S0);
+      slope(Pmm, Pm, P0, rdy, Sm);
+      slope(Pm, P0, P1, rdy, S0);
       if (lane >= 2 && lane <= 29) yface(Pm, Sm, P0, S0, J0 - 1, Gm);
     } else {
       prim_at(J0 - 1, Pm);
       prim_at(J0, P0);
       prim_at(J0 + 1, P1);
-      slope(Pm, P0, P1, dy, S0);
+      slope(Pm, P0, P1, rdy, S0);
 #pragma unroll
       for (int n = 0; n < NV; n++) Gm[n] = 0.0;
     }
@@ -134,7 +136,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
 
   for (int J = J0; J < w.J1; J++) {
     prim_at(J + 2, P2);
-    slope(P0, P1, P2, dy, S1);
+    slope(P0, P1, P2, rdy, S1);
     double G[NV];
     if (lane >= 2 && lane <= 29) yface(P0, S0, P1, S1, J, G);
 
@@ -144,7 +146,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     shfl_down9(P0, Pr);
 #pragma unroll
     for (int n = 0; n < NV; n++) {
-      Sx[n] = limit<LIM>(P0[n] - Pl[n], Pr[n] - P0[n]) / dx;
+      Sx[n] = rdx.div(limit<LIM>(P0[n] - Pl[n], Pr[n] - P0[n]));
       lo[n] = P0[n] + hdx * Sx[n];
       Pl[n] = P0[n] - hdx * Sx[n];
     }

@@ -554,11 +554,15 @@ int orc_steps(orc_ctx *c, double *t, double tend, double CFLmax, double CFLreg,
               double *trace, int trace_cap, int *ntrace)
 {
   int nstep = 0, rej = 0, nt = 0;
+  long attempts = 0;
   double dt = 0.0001, cfl;
   while (*t < tend) {
     if (max_steps > 0 && nstep >= max_steps) break;
     nstep++;
     do {
+      /* the reference loops forever when CFLreg >= CFLmax keeps every retry above
+       * CFLmax; the checker gives up after 10^6 attempts instead (returns -1) */
+      if (++attempts > 1000000L) { if (nrej) *nrej = rej; if (ntrace) *ntrace = nt; return -1; }
       cfl = orc_time_update(c, dt, *t);
       if (cfl > CFLmax) {
         dt = dt * CFLreg / cfl;

@@ -75,7 +75,8 @@ double   orc_time_update(orc_ctx *c, double dt, double t);                   /* 
 
 /* Steps (src/Main.c:189-244).  max_steps > 0 caps the accepted steps (test hook; 0 =
  * no cap).  Every `show_every`-th step appends {step, CFL, t, dt} to trace (if not NULL,
- * up to trace_cap records).  Returns the accepted step count. */
+ * up to trace_cap records).  Returns the accepted step count, or -1 after 10^6
+ * attempts (the reference would loop on forever). */
 int      orc_steps(orc_ctx *c, double *t, double tend, double CFLmax, double CFLreg,
                    int max_steps, int *nrej, int show_every,
                    double *trace, int trace_cap, int *ntrace);
