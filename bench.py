@@ -140,6 +140,48 @@ def run_reference(a, rank):
     print(json.dumps(line), flush=True)
 
 
+def batched_leg(a, local, stream, rank):
+    """Many independent cases: one context advancing all of them in one CUDA-graph
+    loop (per-case dt, one persistent launch per limiter per stage) against the same
+    cases run one after another, each in its own context.  Device time (CUDA events)
+    of the step loops only; context creation and initial states are outside."""
+    import torch
+    from multiblockmomentsfv_b200 import solver as sv
+    cases = sv.batch_workload(seed=a.seed + rank, ncases=a.batch_cases)
+    cells = [d.full_grid_size for d, _ in cases]
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    with sv.BatchSolver(cases, device=local, stream=stream.cuda_stream) as bs:
+        bs.initialise()
+        bs.steps(0.0, 10.0, max_steps=2)
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        _, ns, _ = bs.steps(0.0, 10.0, max_steps=a.batch_steps)
+        e1.record(stream)
+        stream.synchronize()
+        ms_b = e0.elapsed_time(e1)
+        launches = bs.attempts()
+    upd_b = float(sum(c * n for c, n in zip(cells, ns)))
+    ms_s, upd_s = 0.0, 0.0
+    for (d, scn), c in zip(cases, cells):
+        with sv.Solver(d, scn, device=local, show_every=0, stream=stream.cuda_stream) as s1:
+            s1.initialise()
+            s1.steps(0.0, 10.0, max_steps=2)
+            e0, e1 = ev(), ev()
+            e0.record(stream)
+            _, n1, _ = s1.steps(0.0, 10.0, max_steps=a.batch_steps)
+            e1.record(stream)
+            stream.synchronize()
+            ms_s += e0.elapsed_time(e1)
+            upd_s += c * n1
+    return {"cases": len(cases), "steps_per_case": a.batch_steps, "cells": int(sum(cells)),
+            "value": upd_b / (ms_b / 1e3), "serial_value": upd_s / (ms_s / 1e3),
+            "ratio": (upd_b / ms_b) / (upd_s / ms_s), "unit": "cell-updates/s",
+            "ms": ms_b, "serial_ms": ms_s, "graph_attempts": launches,
+            "workload": "64 seeded cases, 1-4 blocks of n x n, n ~ U{64..1024}, Kn log-U[1e-3,1e-1], "
+                        "R13 in {0,1}, limiter ~ U{5}, quadrant state, open edges, 200 steps each, "
+                        "per-case dt; serial = the same cases one context and one Steps loop each"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -152,6 +194,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=50, help="Heun steps per Steps() call in the e2e leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--segment-rows", type=int, default=0)
+    ap.add_argument("--batch-cases", type=int, default=64, help="cases in the batched-vs-serial leg (0 = skip)")
+    ap.add_argument("--batch-steps", type=int, default=200)
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3
@@ -197,6 +241,7 @@ def main():
         e1.record(stream)
         stream.synchronize()
     attempts = s.attempts()
+    launch = s.config()
     ms = e0.elapsed_time(e1)
     barrier()
     ms_max = ms
@@ -251,6 +296,9 @@ def main():
         ms_e2e = float(v[0])
     e2e_value = world * cells * e2e_steps / (ms_e2e / 1e3)
 
+    s.close()
+    batched = batched_leg(a, local, stream, rank) if a.batch_cases > 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         r = cpu_reference(3, 0, 20.0, n=0)
@@ -273,7 +321,7 @@ def main():
                        "cells": cells, "rejected_attempts": nrej,
                        "l2": "working set 3 layers x 4 blocks x 9 planes = "
                              f"{3 * 9 * 8 * sum(b.cells for b in d.blocks) / 1e6:.0f} MB > 126 MB L2, no flush",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}", "launch": launch},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "stage_kernel (Heun stage 1 + stage 2)",
@@ -286,9 +334,9 @@ def main():
             "gpu_launches": 5 * attempts,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
-    s.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

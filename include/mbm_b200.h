@@ -66,6 +66,16 @@ typedef struct {
   void *stream;        /* cudaStream_t to launch on; NULL = a stream the context owns */
 } mbm_params;
 
+/* One independent case of a batch: a contiguous run of blocks of the block array,
+ * with its own physics parameters.  Sync codes of its blocks count from 1 within
+ * the case. */
+typedef struct {
+  int first_block;
+  int nblocks;
+  double Kn, F;
+  int limiter;
+} mbm_case_desc;
+
 typedef struct mbm_ctx mbm_ctx;
 
 /* Allocate device state for a block table.  Replaces the allocation in main()
@@ -73,6 +83,17 @@ typedef struct mbm_ctx mbm_ctx;
  * (src/Boundary.c:101-103) and codes must name existing blocks. */
 int mbm_create(const mbm_block_desc *blocks, int nblocks, const mbm_params *params, mbm_ctx **ctx);
 int mbm_destroy(mbm_ctx *ctx);
+
+/* Many independent cases in one context (no counterpart in the reference, which
+ * runs one case per process): every Heun stage of every case is one persistent
+ * launch per limiter in use, and mbm_steps_batch advances all cases together in
+ * one CUDA-graph loop, each with its own dt, t and step count.  Blocks are indexed
+ * globally in the transfer calls. */
+int mbm_create_batch(const mbm_block_desc *blocks, int nblocks, const mbm_case_desc *cases,
+                     int ncases, const mbm_params *params, mbm_ctx **ctx);
+/* t[c], tend[c], nsteps[c], nrej[c] per case; max_steps > 0 caps accepted steps */
+int mbm_steps_batch(mbm_ctx *ctx, double *t, const double *tend, double CFLmax, double CFLreg,
+                    int max_steps, int *nsteps, int *nrej);
 
 /* Copy one block of a layer between the host (array of structs, (nx+6)*(ny+6)*9
  * doubles, the reference's CVector layer, src/defs.h:42-44) and the device. */
@@ -119,10 +140,17 @@ int mbm_time_stage(mbm_ctx *ctx, int heun, double dt, int reps, double *ms);
 /* Progress records of the last mbm_steps call, one per show_every accepted steps:
  * {step, CFL, t, next dt}, the values the reference prints (src/Main.c:218-230). */
 int mbm_trace(mbm_ctx *ctx, double *records, int cap, int *n);
+/* the same for case c of a batch */
+int mbm_trace_case(mbm_ctx *ctx, int c, double *records, int cap, int *n);
 
 /* Step attempts (accepted + rejected) of the last mbm_steps call; each attempt
  * runs five kernels (two stages, two ghost fills, the controller). */
 int mbm_attempts(mbm_ctx *ctx, int *attempts);
+
+/* Launch configuration in use: rows per warp work item (picked by the autotuner
+ * when mbm_params.segment_rows is 0), work items per stage, CTAs of the persistent
+ * stage grid. */
+int mbm_config(mbm_ctx *ctx, int *segment_rows, int *work_items, int *ctas);
 
 /* Host-only: the resolved ghost-cell sources of a block table, 4 ints per ghost
  * cell {dst_block, dst_cell, src, src_block | flags<<16}; cells are J*(nx+6)+I,

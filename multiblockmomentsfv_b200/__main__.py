@@ -1,0 +1,113 @@
+"""Command line of the reference solver (src/Main.c:61-164) on the GPU path.
+
+    python -m multiblockmomentsfv_b200 -bfile cases/squareSmall.txt -out runs/ss [-double]
+        [-refine n] [-CFL x] [-Kn x] [-R13 x] [-limiter name] [-sfile file]
+        [-scenario riemann2d|ffs|quadrant:SEED|uniform:r,u,v,th] [-device k]
+
+Flags keep the reference's meaning and its quirks: numeric overrides pass through
+``float`` (src/tools.c:38-46), -refine precedes the block file, and -sfile reloads the
+first zones of a result pair into L_DATA with the reference's mapping of the stored
+fields (src/Mesh.c:391-476: the stored pressure p goes where the temperature belongs and
+P_ij where T_ij belongs).  -scenario picks the initial/Dirichlet state that the
+reference hard-codes in src/Scenario.c (default riemann2d).
+"""
+from __future__ import annotations
+
+import os
+import sys
+import time
+
+import numpy as np
+
+from . import blockfile as bf
+from . import output as out
+from . import scenario as sc
+from . import solver as sv
+
+
+def _arg(argv, key, default=None):
+    for i, a in enumerate(argv[1:], 1):
+        if a == key:
+            return argv[i + 1] if i + 1 < len(argv) else None
+    return default
+
+
+def _scenario(spec: str) -> sc.Scenario:
+    if spec.startswith("quadrant:"):
+        return sc.Scenario.seeded_quadrant(int(spec.split(":", 1)[1]))
+    if spec.startswith("uniform:"):
+        v = [float(x) for x in spec.split(":", 1)[1].split(",")]
+        return sc.Scenario(sc.KIND_UNIFORM, [tuple(v)] * 4)
+    return sc.Scenario.named(spec)
+
+
+def load_restart(deck: bf.Deck, path: str):
+    """LoadData (src/Mesh.c:391-476): the first len(blocks) zones fill the interior
+    plus one ghost ring of L_DATA; the remaining cells stay zero."""
+    zones, _ = out.read(path)
+    layers = []
+    for b, z in zip(deck.blocks, zones[:len(deck.blocks)]):
+        U = np.zeros((b.nyp, b.nxp, bf.NV))
+        vals = z["values"].reshape(b.nx + 2, b.ny + 2, 10)      # x outer, y inner
+        P = np.empty((b.nx + 2, b.ny + 2, bf.NV))
+        P[..., 0:3] = vals[..., 0:3]
+        P[..., 3:7] = vals[..., 4:8]
+        P[..., 7:9] = vals[..., 8:10]
+        rho, v1, v2, th = P[..., 0], P[..., 1], P[..., 2], P[..., 3]
+        vs = v1 * v1 + v2 * v2
+        E = 0.5 * rho * vs + 1.5 * rho * th
+        C = np.empty_like(P)
+        C[..., 0] = rho
+        C[..., 1] = rho * v1
+        C[..., 2] = rho * v2
+        C[..., 3] = E
+        C[..., 4] = rho * (P[..., 4] + v1 * v1)
+        C[..., 5] = rho * (P[..., 5] + v1 * v2)
+        C[..., 6] = rho * (P[..., 6] + v2 * v2)
+        C[..., 7] = P[..., 7] + E * v1 + rho * (P[..., 4] * v1 + P[..., 5] * v2)
+        C[..., 8] = P[..., 8] + E * v2 + rho * (P[..., 5] * v1 + P[..., 6] * v2)
+        U[2:b.ny + 4, 2:b.nx + 4, :] = C.transpose(1, 0, 2)
+        layers.append(U)
+    return layers
+
+
+def main(argv=None) -> int:
+    argv = sys.argv if argv is None else argv
+    out_dir = _arg(argv, "-out", "")
+    refine = _arg(argv, "-refine")
+    deck = bf.parse_file(_arg(argv, "-bfile", "blockfile.txt"),
+                         refine=max(1, int(float(refine))) if refine is not None else None)
+    deck = deck.with_cli(Kn=_arg(argv, "-Kn"), R13=_arg(argv, "-R13"), CFL=_arg(argv, "-CFL"),
+                         limiter=_arg(argv, "-limiter"))
+    scn = _scenario(_arg(argv, "-scenario", "riemann2d"))
+    single = "-double" not in argv
+    device = int(_arg(argv, "-device", "0"))
+    print("\n Running: Kn = %.4g, R13 = %g, CFL = %.2f, limiter = %s, BlockFile = \"%s\"" %
+          (deck.Kn, deck.R13, deck.CFL, bf.limiter_name(deck.limiter), _arg(argv, "-bfile", "blockfile.txt")))
+    w = out.Writer(out_dir, deck, scn.type_name, single)
+    sfile = _arg(argv, "-sfile")
+    with sv.Solver(deck, scn, device=device) as s:
+        if sfile:
+            for b, U in enumerate(load_restart(deck, sfile)):
+                s.upload(sv.L_DATA, b, U)
+            s.set_boundary(sv.L_DATA, 0.0)
+        else:
+            s.initialise()
+        w.write(s.layers(), 0.0, -1)
+        t, nmax = 0.0, 0
+        for tn in deck.t_out:
+            t0 = time.perf_counter()
+            t, n, rej = s.steps(t, tn, 1.0, deck.CFL)
+            el = time.perf_counter() - t0
+            for step, cfl, tt, dt in s.trace():
+                print(" step: %3d... done.  CFL: %lf, time: %lf, next dt: %lf" % (step, cfl, tt, dt))
+            print("   %d steps (%d rejected) to t = %g, %.4f us per cell-update" %
+                  (n, rej, t, el * 1e6 / max(1, deck.full_grid_size * (n + rej))))
+            nmax += n
+            w.write(s.layers(), t, nmax)
+    print("\n Done after %d steps.\n" % nmax)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

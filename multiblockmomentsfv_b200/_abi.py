@@ -18,7 +18,8 @@ MODE_EXACT = 0
 EXPORTS = (
     "mbm_create", "mbm_destroy", "mbm_upload", "mbm_download", "mbm_set_dirichlet",
     "mbm_set_boundary", "mbm_update", "mbm_time_update", "mbm_steps", "mbm_steps_capped",
-    "mbm_time_stage", "mbm_trace", "mbm_attempts",
+    "mbm_time_stage", "mbm_trace", "mbm_attempts", "mbm_config",
+    "mbm_create_batch", "mbm_steps_batch", "mbm_trace_case",
     "mbm_ghost_map", "mbm_strerror", "mbm_last_error", "mbm_version",
 )
 
@@ -32,6 +33,11 @@ class Params(C.Structure):
     _fields_ = [("Kn", C.c_double), ("F", C.c_double), ("limiter", C.c_int), ("mode", C.c_int),
                 ("device", C.c_int), ("show_every", C.c_int), ("max_attempts", C.c_int),
                 ("segment_rows", C.c_int), ("stream", C.c_void_p)]
+
+
+class CaseDesc(C.Structure):
+    _fields_ = [("first_block", C.c_int), ("nblocks", C.c_int), ("Kn", C.c_double), ("F", C.c_double),
+                ("limiter", C.c_int)]
 
 
 class MBMError(RuntimeError):
@@ -70,6 +76,10 @@ def lib(path: str = None):
     L.mbm_time_stage.argtypes = [vp, C.c_int, C.c_double, C.c_int, dp]
     L.mbm_trace.argtypes = [vp, dp, C.c_int, P(C.c_int)]
     L.mbm_attempts.argtypes = [vp, P(C.c_int)]
+    L.mbm_config.argtypes = [vp, P(C.c_int), P(C.c_int), P(C.c_int)]
+    L.mbm_create_batch.argtypes = [P(BlockDesc), C.c_int, P(CaseDesc), C.c_int, P(Params), P(vp)]
+    L.mbm_steps_batch.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_int, P(C.c_int), P(C.c_int)]
+    L.mbm_trace_case.argtypes = [vp, C.c_int, dp, C.c_int, P(C.c_int)]
     L.mbm_ghost_map.argtypes = [P(BlockDesc), C.c_int, P(C.c_int), C.c_int, P(C.c_int)]
     L.mbm_strerror.restype = C.c_char_p
     L.mbm_strerror.argtypes = [C.c_int]

@@ -5,6 +5,9 @@
 
 #include <algorithm>
 #include <chrono>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -20,8 +23,10 @@ cudaError_t launch_stage(int lim, const StageArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_ghost(const BlockDev* blk, const CaseDev* cases, const GhostEntry* map, int n,
                          double* const buf[3], const double* dirichlet, int sel, cudaStream_t s);
 cudaError_t launch_control(CaseDev* cases, int ncases, const BlockDev* blk, unsigned long long* lam,
-                           double* trace, cudaGraphConditionalHandle h, int use_handle,
+                           double* trace, int* queues, cudaGraphConditionalHandle h, int use_handle,
                            cudaStream_t s);
+int stage_ctas_per_sm();
+cudaError_t launch_fill_uniform(double* base, long long plane, cudaStream_t s);
 cudaError_t launch_stage_cfl(const BlockDev* blk, int nblk, const CaseDev* cases,
                              unsigned long long* lam, int stage, double* out, cudaStream_t s);
 cudaError_t launch_aos_to_planes(const double* aos, double* dst, int nxp, int nyp, int pitch,
@@ -34,13 +39,18 @@ using namespace mbm;
 
 static thread_local std::string g_create_error;
 
+struct LimGroup {      // the work items of every block whose case uses one limiter
+  int lim, start, count, grid;
+};
+
 struct mbm_ctx {
   mbm_params prm{};
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  int nblk = 0;
-  std::vector<mbm_block_desc> desc;
+  int nblk = 0, ncase = 0;
+  std::vector<mbm_block_desc> desc;  // sync codes global (1-based over all blocks)
+  std::vector<int> blk_case;        // case of each block
   std::vector<BlockDev> hblk;
   BlockDev* dblk = nullptr;
   long long layer_elems = 0;
@@ -53,16 +63,20 @@ struct mbm_ctx {
   int ndir = 0;
   Work* dwork = nullptr;
   int nwork = 0;
-  int grid = 0;
+  std::vector<LimGroup> groups;
+  int nsm = 0, ctas_per_sm = 1;
+  int seg_rows = 0;                 // rows per work item in use
   CaseDev* dcase = nullptr;
-  CaseDev* hcase = nullptr;         // pinned mirror
+  CaseDev* hcase = nullptr;         // pinned mirror, ncase entries
   unsigned long long* dlam = nullptr;
+  int* dqueue = nullptr;            // work counters [stage][limiter]
   double* dtrace = nullptr;
   double* dcfl = nullptr;           // per-block stage CFL for mbm_update
   double* hcfl = nullptr;           // pinned
   cudaEvent_t ev = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
+  bool host_loop = false;           // MBM_HOST_LOOP=1: drive the step loop from the host
   std::string err;
 };
 
@@ -106,16 +120,18 @@ static int wait_stream(mbm_ctx* c) {
 
 static int kind_of(int code) { return code > 0 ? 0 : code == 0 ? 1 : code == -1 ? 2 : 3; }  // sync/open/wall/dirichlet
 
-static int validate(const mbm_block_desc* b, int n, std::string& why) {
+// blocks of a case are [lo, hi); sync codes are global 1-based block numbers here
+static int validate(const mbm_block_desc* b, int n, std::string& why, int lo = 0, int hi = -1) {
   if (!b || n < 1 || n > 65535) { why = "need 1..65535 blocks"; return MBM_EINVAL; }
-  for (int i = 0; i < n; i++) {
+  if (hi < 0) hi = n;
+  for (int i = lo; i < hi; i++) {
     if (b[i].nx < 1 || b[i].ny < 1 || b[i].nx > (1 << 20) || b[i].ny > (1 << 20)) {
       why = "block " + std::to_string(i + 1) + ": bad cell counts"; return MBM_EINVAL;
     }
     if (!(b[i].dx > 0) || !(b[i].dy > 0)) { why = "block " + std::to_string(i + 1) + ": dx, dy must be > 0"; return MBM_EINVAL; }
     for (int s = 0; s < 4; s++) {
       int code = b[i].bc[s];
-      if (code > n) { why = "block " + std::to_string(i + 1) + ": sync partner " + std::to_string(code) + " does not exist"; return MBM_EINVAL; }
+      if (code > 0 && (code - 1 < lo || code - 1 >= hi)) { why = "block " + std::to_string(i + 1) + ": sync partner " + std::to_string(code) + " does not exist"; return MBM_EINVAL; }
       if (code > 0) {  // conforming interface (src/Boundary.c:101-103)
         const mbm_block_desc& p = b[code - 1];
         bool ok = s < 2 ? p.ny == b[i].ny : p.nx == b[i].nx;
@@ -234,37 +250,188 @@ static int resolve_ghosts(const mbm_block_desc* B, int nb, std::vector<Resolved>
 // ------------------------------------------------------------------ create --
 static int pitch_of(int nxp) { return (nxp + 1 + 3) & ~3; }
 
-static int build_work(const std::vector<BlockDev>& blk, int seg_rows, std::vector<Work>& w) {
+// Work items grouped by limiter (the stage kernel is specialised per limiter):
+// blocks of cases with limiter L fill group L, strips within row segments.
+static void build_work(mbm_ctx* c, int seg_rows, std::vector<Work>& w) {
   w.clear();
-  for (int b = 0; b < (int)blk.size(); b++) {
-    const int nxp = blk[b].nxp, nyp = blk[b].nyp;
-    const int nfx = nxp - 3, nfy = nyp - 3;          // face positions 1 .. nxp-3 / nyp-3
-    const int strips = (nfx + STRIP - 1) / STRIP;
-    const int segs = std::max(1, (nfy + seg_rows - 1) / seg_rows);
-    for (int s = 0; s < segs; s++) {
-      // equal-sized segments over face rows [1, nyp-3], the last one reaching nyp-2
-      const int J0 = 1 + (int)((long long)nfy * s / segs);
-      const int J1 = 1 + (int)((long long)nfy * (s + 1) / segs);
-      for (int k = 0; k < strips; k++) w.push_back(Work{b, 1 + STRIP * k, J0, J1});
+  c->groups.clear();
+  for (int lim = 0; lim < 5; lim++) {
+    const int start = (int)w.size();
+    for (int b = 0; b < c->nblk; b++) {
+      if (c->hcase[c->blk_case[b]].limiter != lim) continue;
+      const int nxp = c->hblk[b].nxp, nyp = c->hblk[b].nyp;
+      const int nfx = nxp - 3, nfy = nyp - 3;          // face positions 1 .. nxp-3 / nyp-3
+      const int strips = (nfx + STRIP - 1) / STRIP;
+      const int segs = std::max(1, (nfy + seg_rows - 1) / seg_rows);
+      for (int s = 0; s < segs; s++) {
+        // equal-sized segments over face rows [1, nyp-3], the last one reaching nyp-2
+        const int J0 = 1 + (int)((long long)nfy * s / segs);
+        const int J1 = 1 + (int)((long long)nfy * (s + 1) / segs);
+        for (int k = 0; k < strips; k++) w.push_back(Work{b, 1 + STRIP * k, J0, J1});
+      }
+    }
+    const int count = (int)w.size() - start;
+    if (count > 0) {
+      const int grid = (int)std::min<long long>((count + 3) / 4, (long long)c->nsm * c->ctas_per_sm);
+      c->groups.push_back(LimGroup{lim, start, count, grid});
     }
   }
-  return (int)w.size();
 }
 
-extern "C" int mbm_create(const mbm_block_desc* blocks, int nblocks, const mbm_params* params,
-                          mbm_ctx** out) {
+// rebuild the work table for segments of `seg` rows; the table lives in the same
+// device buffer (sized for 8-row segments)
+static int set_segments(mbm_ctx* c, int seg) {
+  std::vector<Work> work;
+  build_work(c, seg, work);
+  c->nwork = (int)work.size();
+  CK(cudaMemcpyAsync(c->dwork, work.data(), sizeof(Work) * work.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->seg_rows = seg;
+  return MBM_OK;
+}
+
+// one Heun stage of every block: one persistent launch per limiter group
+static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, int sel_out) {
+  for (const LimGroup& g : c->groups) {
+    StageArgs a{};
+    a.blk = c->dblk;
+    a.work = c->dwork + g.start;
+    a.nwork = g.count;
+    a.cases = c->dcase;
+    for (int l = 0; l < 3; l++) a.buf[l] = c->buf[l];
+    a.lam = c->dlam;
+    a.queue = c->dqueue + heun * 5 + g.lim;
+    a.sel_in = sel_in; a.sel_d0 = sel_d0; a.sel_out = sel_out;
+    a.heun = heun;
+    cudaError_t e = launch_stage(g.lim, a, g.grid, c->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// the body of one step attempt: stage 1, fill TMP, stage 2, fill NEW, controller
+static cudaError_t launch_attempt(mbm_ctx* c, cudaGraphConditionalHandle h, int use_handle) {
+  cudaError_t e;
+  if ((e = launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP))) return e;
+  if ((e = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_TMP, c->stream))) return e;
+  if ((e = launch_stages(c, 1, SEL_TMP, SEL_CUR, SEL_OTHER))) return e;
+  if ((e = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_OTHER, c->stream))) return e;
+  return launch_control(c->dcase, c->ncase, c->dblk, c->dlam, c->dtrace, c->dqueue, h, use_handle, c->stream);
+}
+
+static int push_cases(mbm_ctx* c) {
+  CK(cudaMemcpyAsync(c->dcase, c->hcase, sizeof(CaseDev) * c->ncase, cudaMemcpyHostToDevice, c->stream));
+  return MBM_OK;
+}
+
+// Autotuner: the stage kernel's work-item length (rows per warp segment) trades
+// the per-segment warm-up (two extra primitive rows, one slope row, one face row)
+// against load balance over the persistent grid.  On first use of a problem shape
+// it times both Heun stages for each candidate on a uniform state at rest and keeps
+// the fastest; the choice is cached per (strip rows, blocks, limiter mix, CTAs/SM)
+// for the life of the process.
+static std::mutex g_tune_mu;
+static std::map<std::tuple<long long, int, int, int>, int> g_tune_cache;
+
+static int time_both_stages(mbm_ctx* c, cudaEvent_t e0, cudaEvent_t e1, float* ms) {
+  for (int rep = 0; rep < 3; rep++) {
+    if (rep == 1) CK(cudaEventRecord(e0, c->stream));
+    for (int heun = 0; heun < 2; heun++) {
+      CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
+      CK(launch_stages(c, heun, heun ? SEL_TMP : SEL_CUR, SEL_CUR, heun ? SEL_OTHER : SEL_TMP));
+    }
+  }
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  CK(cudaEventElapsedTime(ms, e0, e1));
+  return MBM_OK;
+}
+
+static int autotune(mbm_ctx* c) {
+  long long strip_rows = 0, cells = 0;
+  for (auto& d : c->hblk) {
+    strip_rows += (long long)((d.nxp - 3 + STRIP - 1) / STRIP) * (d.nyp - 3);
+    cells += (long long)d.nxp * d.nyp;
+  }
+  int limmix = 0;
+  for (const LimGroup& g : c->groups) limmix |= 1 << g.lim;
+  const auto key = std::make_tuple(strip_rows, c->nblk, limmix, c->ctas_per_sm);
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) return set_segments(c, it->second);
+  }
+  const char* env = getenv("MBM_AUTOTUNE");
+  if ((env && atoi(env) == 0) || cells < 200000) return set_segments(c, 32);
+  for (int l = 0; l < 3; l++)
+    for (auto& d : c->hblk) CK(launch_fill_uniform(c->buf[l] + d.off, d.plane, c->stream));
+  for (int k = 0; k < c->ncase; k++) {
+    c->hcase[k].dt = 1e-5;
+    c->hcase[k].done = 0;
+  }
+  int st = push_cases(c);
+  if (st) return st;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int best = 32;
+  float best_ms = 1e30f;
+  for (int seg : {16, 24, 32, 48, 64, 96}) {
+    st = set_segments(c, seg);
+    float ms = 0.f;
+    if (!st) st = time_both_stages(c, e0, e1, &ms);
+    if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
+    if (ms < best_ms) { best_ms = ms; best = seg; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (int l = 0; l < 3; l++) CK(cudaMemsetAsync(c->buf[l], 0, sizeof(double) * c->layer_elems, c->stream));
+  CK(cudaMemsetAsync(c->dlam, 0, sizeof(unsigned long long) * 6 * c->nblk, c->stream));
+  for (int k = 0; k < c->ncase; k++) c->hcase[k].done = 1;
+  if ((st = push_cases(c))) return st;
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune_cache[key] = best;
+  }
+  return set_segments(c, best);
+}
+
+extern "C" int mbm_create_batch(const mbm_block_desc* blocks, int nblocks, const mbm_case_desc* cases,
+                                int ncases, const mbm_params* params, mbm_ctx** out) {
   mbm_ctx* c = nullptr;
-  if (!out || !params) return fail(nullptr, MBM_EINVAL, "null argument");
+  if (!out || !params || !cases || ncases < 1) return fail(nullptr, MBM_EINVAL, "null argument");
   *out = nullptr;
   std::string why;
-  if (validate(blocks, nblocks, why) != MBM_OK) return fail(nullptr, MBM_EINVAL, why);
-  if (params->limiter < 0 || params->limiter > 4) return fail(nullptr, MBM_EINVAL, "limiter code must be 0..4");
+  if (!blocks || nblocks < 1 || nblocks > 65535) return fail(nullptr, MBM_EINVAL, "need 1..65535 blocks");
   if (params->mode != MBM_MODE_EXACT) return fail(nullptr, MBM_EINVAL, "unknown arithmetic mode");
-  if (!(params->Kn > 0)) return fail(nullptr, MBM_EINVAL, "Kn must be > 0");
+  // cases tile the block array; sync codes become global block numbers
+  std::vector<mbm_block_desc> glob(blocks, blocks + nblocks);
+  std::vector<int> blk_case(nblocks, -1);
+  for (int k = 0; k < ncases; k++) {
+    const mbm_case_desc& cd = cases[k];
+    if (cd.nblocks < 1 || cd.first_block < 0 || cd.first_block + cd.nblocks > nblocks)
+      return fail(nullptr, MBM_EINVAL, "case " + std::to_string(k) + ": block range outside the table");
+    if (cd.limiter < 0 || cd.limiter > 4) return fail(nullptr, MBM_EINVAL, "limiter code must be 0..4");
+    if (!(cd.Kn > 0)) return fail(nullptr, MBM_EINVAL, "Kn must be > 0");
+    for (int b = cd.first_block; b < cd.first_block + cd.nblocks; b++) {
+      if (blk_case[b] >= 0) return fail(nullptr, MBM_EINVAL, "cases overlap");
+      blk_case[b] = k;
+      for (int s = 0; s < 4; s++)
+        if (glob[b].bc[s] > 0) {
+          if (glob[b].bc[s] > cd.nblocks)
+            return fail(nullptr, MBM_EINVAL, "case " + std::to_string(k) + ": sync partner outside the case");
+          glob[b].bc[s] += cd.first_block;
+        }
+    }
+    if (validate(glob.data(), nblocks, why, cd.first_block, cd.first_block + cd.nblocks) != MBM_OK)
+      return fail(nullptr, MBM_EINVAL, "case " + std::to_string(k) + ": " + why);
+  }
+  for (int b = 0; b < nblocks; b++)
+    if (blk_case[b] < 0) return fail(nullptr, MBM_EINVAL, "block " + std::to_string(b + 1) + " belongs to no case");
   std::vector<Resolved> res;
   std::vector<int> dir_off;
   int ndir = 0;
-  if (resolve_ghosts(blocks, nblocks, res, dir_off, ndir, why) != MBM_OK)
+  if (resolve_ghosts(glob.data(), nblocks, res, dir_off, ndir, why) != MBM_OK)
     return fail(nullptr, MBM_EINVAL, why);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(nullptr, MBM_ENODEV, "no CUDA device");
@@ -272,10 +439,16 @@ extern "C" int mbm_create(const mbm_block_desc* blocks, int nblocks, const mbm_p
 
   c = new mbm_ctx();
   c->prm = *params;
+  {
+    const char* hl = getenv("MBM_HOST_LOOP");
+    c->host_loop = hl && atoi(hl) != 0;
+  }
   if (c->prm.max_attempts <= 0) c->prm.max_attempts = 10000000;
   c->device = params->device;
   c->nblk = nblocks;
-  c->desc.assign(blocks, blocks + nblocks);
+  c->ncase = ncases;
+  c->desc = glob;
+  c->blk_case = blk_case;
   c->dir_off = dir_off;
   c->ndir = ndir;
   auto bail = [&](int code) { g_create_error = c->err; mbm_destroy(c); return code; };
@@ -300,14 +473,14 @@ extern "C" int mbm_create(const mbm_block_desc* blocks, int nblocks, const mbm_p
   long long off = 0, max_cells = 0;
   for (int b = 0; b < nblocks; b++) {
     BlockDev d{};
-    d.nxp = blocks[b].nx + 2 * NG;
-    d.nyp = blocks[b].ny + 2 * NG;
+    d.nxp = glob[b].nx + 2 * NG;
+    d.nyp = glob[b].ny + 2 * NG;
     d.pitch = pitch_of(d.nxp);
-    d.case_id = 0;
+    d.case_id = blk_case[b];
     d.plane = ((long long)d.pitch * d.nyp + 31) & ~31LL;
     d.off = off;
-    d.dx = blocks[b].dx;
-    d.dy = blocks[b].dy;
+    d.dx = glob[b].dx;
+    d.dy = glob[b].dy;
     off += d.plane * NV;
     max_cells = std::max(max_cells, (long long)d.nxp * d.nyp);
     c->hblk.push_back(d);
@@ -345,41 +518,40 @@ extern "C" int mbm_create(const mbm_block_desc* blocks, int nblocks, const mbm_p
   CKC(cudaMalloc(&c->ddir, sizeof(double) * NV * std::max(1, ndir)));
   CKC(cudaMemsetAsync(c->ddir, 0, sizeof(double) * NV * std::max(1, ndir), c->stream));
 
-  // work table and grid
-  int sm = 0, per_sm = 0;
-  CKC(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, c->device));
-  per_sm = 4;
-  long long strip_rows = 0;
-  for (auto& d : c->hblk) strip_rows += (long long)((d.nxp - 3 + STRIP - 1) / STRIP) * (d.nyp - 3);
-  int seg = params->segment_rows;
-  if (seg <= 0) {
-    const long long target = 2LL * sm * per_sm * 4;   // two warp items per resident warp
-    seg = (int)std::max<long long>(32, (strip_rows + target - 1) / target);
+  // controllers, maxima, queues, trace, per-block CFL
+  CKC(cudaMalloc(&c->dcase, sizeof(CaseDev) * ncases));
+  CKC(cudaMallocHost(&c->hcase, sizeof(CaseDev) * ncases));
+  memset(c->hcase, 0, sizeof(CaseDev) * ncases);
+  for (int k = 0; k < ncases; k++) {
+    CaseDev& h = c->hcase[k];
+    h.Kn = cases[k].Kn;
+    h.F = cases[k].F;
+    h.limiter = cases[k].limiter;
+    h.cur = 0;
+    h.done = 1;
+    h.blk0 = cases[k].first_block;
+    h.nblk = cases[k].nblocks;
+    h.max_attempts = c->prm.max_attempts;
   }
-  std::vector<Work> work;
-  c->nwork = build_work(c->hblk, seg, work);
-  CKC(cudaMalloc(&c->dwork, sizeof(Work) * work.size()));
-  CKC(cudaMemcpyAsync(c->dwork, work.data(), sizeof(Work) * work.size(), cudaMemcpyHostToDevice, c->stream));
-  c->grid = (int)std::min<long long>((c->nwork + 3) / 4, (long long)sm * per_sm);
-
-  // controller, maxima, trace, per-block CFL
-  CKC(cudaMalloc(&c->dcase, sizeof(CaseDev)));
-  CKC(cudaMallocHost(&c->hcase, sizeof(CaseDev)));
-  memset(c->hcase, 0, sizeof(CaseDev));
-  c->hcase->Kn = params->Kn;
-  c->hcase->F = params->F;
-  c->hcase->limiter = params->limiter;
-  c->hcase->cur = 0;
-  c->hcase->done = 1;
-  c->hcase->blk0 = 0;
-  c->hcase->nblk = nblocks;
-  c->hcase->max_attempts = c->prm.max_attempts;
-  CKC(cudaMemcpyAsync(c->dcase, c->hcase, sizeof(CaseDev), cudaMemcpyHostToDevice, c->stream));
+  CKC(cudaMemcpyAsync(c->dcase, c->hcase, sizeof(CaseDev) * ncases, cudaMemcpyHostToDevice, c->stream));
+  CKC(cudaMalloc(&c->dqueue, sizeof(int) * 10));
+  CKC(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
   CKC(cudaMalloc(&c->dlam, sizeof(unsigned long long) * 6 * nblocks));
   CKC(cudaMemsetAsync(c->dlam, 0, sizeof(unsigned long long) * 6 * nblocks, c->stream));
-  CKC(cudaMalloc(&c->dtrace, sizeof(double) * 4 * MAX_TRACE));
+  CKC(cudaMalloc(&c->dtrace, sizeof(double) * 4 * MAX_TRACE * ncases));
   CKC(cudaMalloc(&c->dcfl, sizeof(double) * nblocks));
   CKC(cudaMallocHost(&c->hcfl, sizeof(double) * nblocks));
+
+  // work table and grid
+  CKC(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device));
+  c->ctas_per_sm = stage_ctas_per_sm();
+  long long max_items = 0;
+  for (auto& d : c->hblk) max_items += (long long)((d.nxp - 3 + STRIP - 1) / STRIP) * ((d.nyp - 3 + 7) / 8 + 1);
+  CKC(cudaMalloc(&c->dwork, sizeof(Work) * std::max<long long>(1, max_items)));
+  {
+    int st0 = params->segment_rows > 0 ? set_segments(c, std::max(8, params->segment_rows)) : autotune(c);
+    if (st0) return bail(st0);
+  }
 
   // the step loop: while (any case live) { stage 1; fill TMP; stage 2; fill NEW; control }
   {
@@ -395,20 +567,10 @@ extern "C" int mbm_create(const mbm_block_desc* blocks, int nblocks, const mbm_p
     CKC(cudaGraphAddNode(&node, c->graph, nullptr, 0, &np));
     cudaGraph_t body = np.conditional.phGraph_out[0];
     CKC(cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    StageArgs a{};
-    a.blk = c->dblk; a.work = c->dwork; a.nwork = c->nwork; a.cases = c->dcase;
-    for (int l = 0; l < 3; l++) a.buf[l] = c->buf[l];
-    a.lam = c->dlam;
-    a.sel_in = SEL_CUR; a.sel_d0 = SEL_CUR; a.sel_out = SEL_TMP; a.heun = 0;
-    cudaError_t e1 = launch_stage(params->limiter, a, c->grid, c->stream);
-    cudaError_t e2 = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_TMP, c->stream);
-    a.sel_in = SEL_TMP; a.sel_d0 = SEL_CUR; a.sel_out = SEL_OTHER; a.heun = 1;
-    cudaError_t e3 = launch_stage(params->limiter, a, c->grid, c->stream);
-    cudaError_t e4 = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_OTHER, c->stream);
-    cudaError_t e5 = launch_control(c->dcase, 1, c->dblk, c->dlam, c->dtrace, h, 1, c->stream);
+    cudaError_t e1 = launch_attempt(c, h, 1);
     cudaGraph_t captured = nullptr;
     CKC(cudaStreamEndCapture(c->stream, &captured));
-    CKC(e1); CKC(e2); CKC(e3); CKC(e4); CKC(e5);
+    CKC(e1);
     CKC(cudaGraphInstantiate(&c->gexec, c->graph, 0));
   }
   int st = wait_stream(c);
@@ -416,6 +578,18 @@ extern "C" int mbm_create(const mbm_block_desc* blocks, int nblocks, const mbm_p
   *out = c;
   return MBM_OK;
 #undef CKC
+}
+
+extern "C" int mbm_create(const mbm_block_desc* blocks, int nblocks, const mbm_params* params,
+                          mbm_ctx** out) {
+  if (!params) return fail(nullptr, MBM_EINVAL, "null argument");
+  mbm_case_desc one;
+  one.first_block = 0;
+  one.nblocks = nblocks;
+  one.Kn = params->Kn;
+  one.F = params->F;
+  one.limiter = params->limiter;
+  return mbm_create_batch(blocks, nblocks, &one, 1, params, out);
 }
 
 extern "C" int mbm_destroy(mbm_ctx* c) {
@@ -433,6 +607,7 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   cudaFree(c->dcase);
   if (c->hcase) cudaFreeHost(c->hcase);
   cudaFree(c->dlam);
+  cudaFree(c->dqueue);
   cudaFree(c->dtrace);
   cudaFree(c->dcfl);
   if (c->hcfl) cudaFreeHost(c->hcfl);
@@ -449,13 +624,16 @@ static int layer_sel(int layer) {
 
 static bool bad_layer(int layer) { return layer < 0 || layer > 2; }
 
+static int phys_of(mbm_ctx* c, int layer, int block) {
+  return phys_layer(layer_sel(layer), c->hcase[c->blk_case[block]].cur);
+}
+
 extern "C" int mbm_upload(mbm_ctx* c, int layer, int block, const double* cells) {
   if (!c || !cells || bad_layer(layer) || block < 0 || block >= c->nblk) return fail(c, MBM_EINVAL, "mbm_upload: bad argument");
   CK(cudaSetDevice(c->device));
   const BlockDev& d = c->hblk[block];
-  const int phys = phys_layer(layer_sel(layer), c->hcase->cur);
   CK(cudaMemcpyAsync(c->staging, cells, sizeof(double) * d.nxp * d.nyp * NV, cudaMemcpyHostToDevice, c->stream));
-  CK(launch_aos_to_planes(c->staging, c->buf[phys] + d.off, d.nxp, d.nyp, d.pitch, d.plane, c->stream));
+  CK(launch_aos_to_planes(c->staging, c->buf[phys_of(c, layer, block)] + d.off, d.nxp, d.nyp, d.pitch, d.plane, c->stream));
   return wait_stream(c);
 }
 
@@ -463,8 +641,7 @@ extern "C" int mbm_download(mbm_ctx* c, int layer, int block, double* cells) {
   if (!c || !cells || bad_layer(layer) || block < 0 || block >= c->nblk) return fail(c, MBM_EINVAL, "mbm_download: bad argument");
   CK(cudaSetDevice(c->device));
   const BlockDev& d = c->hblk[block];
-  const int phys = phys_layer(layer_sel(layer), c->hcase->cur);
-  CK(launch_planes_to_aos(c->buf[phys] + d.off, c->staging, d.nxp, d.nyp, d.pitch, d.plane, c->stream));
+  CK(launch_planes_to_aos(c->buf[phys_of(c, layer, block)] + d.off, c->staging, d.nxp, d.nyp, d.pitch, d.plane, c->stream));
   CK(cudaMemcpyAsync(cells, c->staging, sizeof(double) * d.nxp * d.nyp * NV, cudaMemcpyDeviceToHost, c->stream));
   return wait_stream(c);
 }
@@ -481,30 +658,28 @@ extern "C" int mbm_set_dirichlet(mbm_ctx* c, int block, int side, const double* 
 }
 
 // ------------------------------------------------------------- stage calls --
-static int push_case(mbm_ctx* c) {
-  CK(cudaMemcpyAsync(c->dcase, c->hcase, sizeof(CaseDev), cudaMemcpyHostToDevice, c->stream));
-  return MBM_OK;
+static void live_all(mbm_ctx* c, double dt, double t) {
+  for (int k = 0; k < c->ncase; k++) {
+    c->hcase[k].dt = dt;
+    c->hcase[k].t = t;
+    c->hcase[k].done = 0;
+  }
 }
 
 extern "C" int mbm_set_boundary(mbm_ctx* c, int layer, double t) {
   (void)t;   // Dirichlet values are the host-set table; the reference's states are steady
   if (!c || bad_layer(layer)) return fail(c, MBM_EINVAL, "mbm_set_boundary: bad argument");
   CK(cudaSetDevice(c->device));
-  c->hcase->done = 0;
-  int st = push_case(c);
+  for (int k = 0; k < c->ncase; k++) c->hcase[k].done = 0;
+  int st = push_cases(c);
   if (st) return st;
   CK(launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, layer_sel(layer), c->stream));
   return wait_stream(c);
 }
 
 static int run_stage(mbm_ctx* c, int out_layer, int in_layer, int d0_layer, int heun, double* cfl) {
-  StageArgs a{};
-  a.blk = c->dblk; a.work = c->dwork; a.nwork = c->nwork; a.cases = c->dcase;
-  for (int l = 0; l < 3; l++) a.buf[l] = c->buf[l];
-  a.lam = c->dlam;
-  a.sel_in = layer_sel(in_layer); a.sel_d0 = layer_sel(d0_layer); a.sel_out = layer_sel(out_layer);
-  a.heun = heun;
-  CK(launch_stage(c->prm.limiter, a, c->grid, c->stream));
+  CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
+  CK(launch_stages(c, heun, layer_sel(in_layer), layer_sel(d0_layer), layer_sel(out_layer)));
   CK(launch_stage_cfl(c->dblk, c->nblk, c->dcase, c->dlam, heun, c->dcfl, c->stream));
   CK(cudaMemcpyAsync(c->hcfl, c->dcfl, sizeof(double) * c->nblk, cudaMemcpyDeviceToHost, c->stream));
   int st = wait_stream(c);
@@ -519,10 +694,8 @@ extern "C" int mbm_update(mbm_ctx* c, int out_layer, int in_layer, int data0_lay
       out_layer == in_layer || out_layer == data0_layer)
     return fail(c, MBM_EINVAL, "mbm_update: bad argument");
   CK(cudaSetDevice(c->device));
-  c->hcase->dt = dt;
-  c->hcase->t = t;
-  c->hcase->done = 0;
-  int st = push_case(c);
+  live_all(c, dt, t);
+  int st = push_cases(c);
   if (st) return st;
   return run_stage(c, out_layer, in_layer, data0_layer, heun, cfl);
 }
@@ -543,34 +716,73 @@ extern "C" int mbm_time_update(mbm_ctx* c, double dt, double t, double* cfl) {
   return MBM_OK;
 }
 
+// Steps for every case at once: each case has its own t, tend and dt; the loop
+// ends when every case is done (t >= tend, max_steps reached, or a failure).
+extern "C" int mbm_steps_batch(mbm_ctx* c, double* t, const double* tend, double CFLmax, double CFLreg,
+                               int max_steps, int* nsteps, int* nrej) {
+  if (!c || !t || !tend || max_steps < 0) return fail(c, MBM_EINVAL, "mbm_steps: bad argument");
+  CK(cudaSetDevice(c->device));
+  bool any = false;
+  for (int k = 0; k < c->ncase; k++) {
+    CaseDev& h = c->hcase[k];
+    h.t = t[k];
+    h.tend = tend[k];
+    h.dt = 0.0001;               // DT_INITIAL, reset on every call (src/Main.c:28,193)
+    h.CFLmax = CFLmax;
+    h.CFLreg = CFLreg;
+    h.nstep = h.nrej = h.attempts = 0;
+    h.step_cap = max_steps;
+    h.status = 0;
+    h.trace_n = 0;
+    h.show_every = c->prm.show_every;
+    h.max_attempts = c->prm.max_attempts;
+    h.done = (t[k] < tend[k]) ? 0 : 1;
+    any = any || !h.done;
+  }
+  int st = push_cases(c);
+  if (st) return st;
+  if (any && !c->host_loop) {
+    CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
+    CK(cudaGraphLaunch(c->gexec, c->stream));
+  } else if (any) {
+    // the graph body launched from the host, 16 attempts between checks of the
+    // controller state (kernels of finished cases return at once); for tools that
+    // cannot look inside conditional graph nodes
+    CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
+    for (;;) {
+      for (int k = 0; k < 16; k++) CK(launch_attempt(c, 0, 0));
+      CK(cudaMemcpyAsync(c->hcase, c->dcase, sizeof(CaseDev) * c->ncase, cudaMemcpyDeviceToHost, c->stream));
+      if ((st = wait_stream(c))) return st;
+      bool live = false;
+      for (int k = 0; k < c->ncase; k++) live = live || !c->hcase[k].done;
+      if (!live) break;
+    }
+  }
+  CK(cudaMemcpyAsync(c->hcase, c->dcase, sizeof(CaseDev) * c->ncase, cudaMemcpyDeviceToHost, c->stream));
+  if ((st = wait_stream(c))) return st;
+  int worst = 0;
+  for (int k = 0; k < c->ncase; k++) {
+    const CaseDev& h = c->hcase[k];
+    t[k] = h.t;
+    if (nsteps) nsteps[k] = h.nstep;
+    if (nrej) nrej[k] = h.nrej;
+    if (h.status) worst = h.status;
+  }
+  if (worst == 2) return fail(c, MBM_ENONFINITE, "CFL or dt became non-finite");
+  if (worst == 5) return fail(c, MBM_ESTEPLIMIT, "step attempts exceeded max_attempts");
+  return MBM_OK;
+}
+
 extern "C" int mbm_steps_capped(mbm_ctx* c, double* t, double tend, double CFLmax, double CFLreg,
                                 int max_steps, int* nsteps, int* nrej) {
-  if (!c || !t || max_steps < 0) return fail(c, MBM_EINVAL, "mbm_steps: bad argument");
-  CK(cudaSetDevice(c->device));
-  CaseDev& h = *c->hcase;
-  h.t = *t;
-  h.tend = tend;
-  h.dt = 0.0001;                 // DT_INITIAL, reset on every call (src/Main.c:28,193)
-  h.CFLmax = CFLmax;
-  h.CFLreg = CFLreg;
-  h.nstep = h.nrej = h.attempts = 0;
-  h.step_cap = max_steps;
-  h.status = 0;
-  h.trace_n = 0;
-  h.show_every = c->prm.show_every;
-  h.max_attempts = c->prm.max_attempts;
-  h.done = (*t < tend) ? 0 : 1;
-  int st = push_case(c);
-  if (st) return st;
-  if (!h.done) CK(cudaGraphLaunch(c->gexec, c->stream));
-  CK(cudaMemcpyAsync(c->hcase, c->dcase, sizeof(CaseDev), cudaMemcpyDeviceToHost, c->stream));
-  if ((st = wait_stream(c))) return st;
-  *t = h.t;
-  if (nsteps) *nsteps = h.nstep;
-  if (nrej) *nrej = h.nrej;
-  if (h.status == 2) return fail(c, MBM_ENONFINITE, "CFL or dt became non-finite");
-  if (h.status == 5) return fail(c, MBM_ESTEPLIMIT, "step attempts exceeded max_attempts");
-  return MBM_OK;
+  if (!c || !t) return fail(c, MBM_EINVAL, "mbm_steps: bad argument");
+  std::vector<double> tt(c->ncase, *t), te(c->ncase, tend);
+  std::vector<int> ns(c->ncase), nr(c->ncase);
+  int st = mbm_steps_batch(c, tt.data(), te.data(), CFLmax, CFLreg, max_steps, ns.data(), nr.data());
+  *t = tt[0];
+  if (nsteps) *nsteps = ns[0];
+  if (nrej) *nrej = nr[0];
+  return st;
 }
 
 extern "C" int mbm_steps(mbm_ctx* c, double* t, double tend, double CFLmax, double CFLreg, int* nsteps,
@@ -578,32 +790,45 @@ extern "C" int mbm_steps(mbm_ctx* c, double* t, double tend, double CFLmax, doub
   return mbm_steps_capped(c, t, tend, CFLmax, CFLreg, 0, nsteps, nrej);
 }
 
+extern "C" int mbm_config(mbm_ctx* c, int* segment_rows, int* work_items, int* ctas) {
+  if (!c) return fail(c, MBM_EINVAL, "mbm_config: null context");
+  int g = 0;
+  for (const LimGroup& x : c->groups) g = std::max(g, x.grid);
+  if (segment_rows) *segment_rows = c->seg_rows;
+  if (work_items) *work_items = c->nwork;
+  if (ctas) *ctas = g;
+  return MBM_OK;
+}
+
 extern "C" int mbm_attempts(mbm_ctx* c, int* attempts) {
   if (!c || !attempts) return fail(c, MBM_EINVAL, "mbm_attempts: bad argument");
-  *attempts = c->hcase->attempts;
+  int a = 0;
+  for (int k = 0; k < c->ncase; k++) a = std::max(a, c->hcase[k].attempts);
+  *attempts = a;
   return MBM_OK;
 }
 
 extern "C" int mbm_time_stage(mbm_ctx* c, int heun, double dt, int reps, double* ms) {
   if (!c || !ms || reps < 1 || (heun != 0 && heun != 1)) return fail(c, MBM_EINVAL, "mbm_time_stage: bad argument");
   CK(cudaSetDevice(c->device));
-  c->hcase->dt = dt;
-  c->hcase->done = 0;
-  int st = push_case(c);
+  for (int k = 0; k < c->ncase; k++) {
+    c->hcase[k].dt = dt;
+    c->hcase[k].done = 0;
+  }
+  int st = push_cases(c);
   if (st) return st;
-  StageArgs a{};
-  a.blk = c->dblk; a.work = c->dwork; a.nwork = c->nwork; a.cases = c->dcase;
-  for (int l = 0; l < 3; l++) a.buf[l] = c->buf[l];
-  a.lam = c->dlam;
-  a.heun = heun;
-  if (heun == 0) { a.sel_in = SEL_CUR; a.sel_d0 = SEL_CUR; a.sel_out = SEL_TMP; }
-  else { a.sel_in = SEL_TMP; a.sel_d0 = SEL_CUR; a.sel_out = SEL_OTHER; }
+  const int si = heun ? SEL_TMP : SEL_CUR, so = heun ? SEL_OTHER : SEL_TMP;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  CK(launch_stage(c->prm.limiter, a, c->grid, c->stream));      // warm-up launch
+  CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
+  CK(launch_stages(c, heun, si, SEL_CUR, so));      // warm-up launch
+  // the per-launch queue reset is a 40-byte memset, inside the timed region
   CK(cudaEventRecord(e0, c->stream));
-  for (int r = 0; r < reps; r++) CK(launch_stage(c->prm.limiter, a, c->grid, c->stream));
+  for (int r = 0; r < reps; r++) {
+    CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
+    CK(launch_stages(c, heun, si, SEL_CUR, so));
+  }
   CK(cudaEventRecord(e1, c->stream));
   CK(launch_stage_cfl(c->dblk, c->nblk, c->dcase, c->dlam, heun, c->dcfl, c->stream));
   st = wait_stream(c);
@@ -617,13 +842,17 @@ extern "C" int mbm_time_stage(mbm_ctx* c, int heun, double dt, int reps, double*
 }
 
 extern "C" int mbm_trace(mbm_ctx* c, double* rec, int cap, int* n) {
-  if (!c || (cap > 0 && !rec)) return fail(c, MBM_EINVAL, "mbm_trace: bad argument");
-  const int k = std::min(cap, c->hcase->trace_n);
-  if (k > 0) {
+  return mbm_trace_case(c, 0, rec, cap, n);
+}
+
+extern "C" int mbm_trace_case(mbm_ctx* c, int k, double* rec, int cap, int* n) {
+  if (!c || k < 0 || k >= c->ncase || (cap > 0 && !rec)) return fail(c, MBM_EINVAL, "mbm_trace: bad argument");
+  const int m = std::min(cap, c->hcase[k].trace_n);
+  if (m > 0) {
     CK(cudaSetDevice(c->device));
-    CK(cudaMemcpy(rec, c->dtrace, sizeof(double) * 4 * k, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(rec, c->dtrace + (size_t)k * MAX_TRACE * 4, sizeof(double) * 4 * m, cudaMemcpyDeviceToHost));
   }
-  if (n) *n = k;
+  if (n) *n = m;
   return MBM_OK;
 }
 

@@ -61,6 +61,7 @@ struct StageArgs {
   CaseDev* cases;
   double* buf[3];
   unsigned long long* lam;   // [block][stage][3]: max lambda_x, lambda_y, CFL_prod bits
+  int* queue;                // work-item counter of this stage (zero before the launch)
   int sel_in, sel_d0, sel_out;
   int heun;
 };

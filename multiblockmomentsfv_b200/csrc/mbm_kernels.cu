@@ -21,19 +21,6 @@
 
 namespace mbm {
 
-__device__ __forceinline__ void shfl_up9(const double (&a)[NV], double (&b)[NV]) {
-#pragma unroll
-  for (int n = 0; n < NV; n++) b[n] = __shfl_up_sync(0xffffffffu, a[n], 1);
-}
-__device__ __forceinline__ void shfl_down9(const double (&a)[NV], double (&b)[NV]) {
-#pragma unroll
-  for (int n = 0; n < NV; n++) b[n] = __shfl_down_sync(0xffffffffu, a[n], 1);
-}
-__device__ __forceinline__ void copy9(const double (&a)[NV], double (&b)[NV]) {
-#pragma unroll
-  for (int n = 0; n < NV; n++) b[n] = a[n];
-}
-
 // moments of a state at rest with rho = theta = 1: fed to lanes and rows that fall
 // outside the padded grid, whose results are never used
 __device__ __forceinline__ void benign(double (&U)[NV]) {
@@ -47,8 +34,22 @@ __device__ __forceinline__ void load_cell(const double* __restrict__ base, long 
   for (int n = 0; n < NV; n++) U[n] = __ldg(base + n * plane + idx);
 }
 
+// Rolling state of one warp, lane fastest (conflict-free 8-byte accesses): the
+// projected primitives of three consecutive rows, the lower state of the next
+// y face and the y flux of the face below the row being finished.
+struct WarpWindow {
+  double P[3][NV][32];
+  double lo[NV][32];
+  double G[NV][32];
+};
+constexpr int STAGE_WARPS = 4;
+#ifndef STAGE_MIN_CTAS
+#define STAGE_MIN_CTAS 3   // CTAs per SM the register budget is sized for (168 registers)
+#endif
+
 template <int HEUN, int LIM>
-__device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, const int lane) {
+__device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, const int lane,
+                                           WarpWindow& win) {
   const BlockDev B = a.blk[w.blk];
   const CaseDev& cs = a.cases[B.case_id];
   if (cs.done) return;
@@ -66,127 +67,118 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   const bool col_face = C >= 1 && C <= nxp - 3;      // face loop range (src/Main.c:353-354)
   const bool col_cell = C >= 1 && C <= nxp - 2;      // relaxation range (src/Main.c:320-321)
   const bool col_out = lane >= 2 && lane <= 29 && C >= NG && C <= nxp - 1 - NG;
-  const double dx = B.dx, dy = B.dy;
-  const double dtdx = dt / dx, dtdy = dt / dy;
-  const Recip rdx(dx), rdy(dy);
-  const double hdx = 0.5 * dx, hdy = 0.5 * dy;
+  const bool ylane = lane >= 2 && lane <= 29;        // owners of this strip's y faces
+  const double dtdx = dt / B.dx, dtdy = dt / B.dy;
+  const Recip rdx(B.dx), rdy(B.dy);
+  const double hdx = 0.5 * B.dx, hdy = 0.5 * B.dy;
   double lamx = 0.0, lamy = 0.0, prod = 0.0;
 
-  // projected primitives of cell (C, J): Aux.Prim after src/Main.c:314-336
-  auto prim_at = [&](int J, double (&P)[NV]) {
-    double U[NV], Q[NV];
-    const bool ok = col_in && J >= 0 && J < nyp;
-    if (ok) load_cell(in, plane, (long long)J * pitch + C + 1, U);
-    else benign(U);
-    primitive(U, Q);
-    const bool ring = col_ring || J == 0 || J == nyp - 1;
-    if (ok && col_cell && J >= 1 && J <= nyp - 2) {
-      const double c = relax_cfl<2 * HEUN>(Q, dt, Kn);
-      if (c > prod) prod = c;
-    }
-    if (ring) {
-      copy9(Q, P);
-    } else {
-      double V[NV];
-      relax<2 * HEUN + 1>(Q, V, dt, Kn, Fx);
-      primitive(V, P);
-    }
-  };
-  // y slope from three consecutive rows (src/Main.c:348-349)
-  auto slope = [&](const double (&Pm)[NV], const double (&P0)[NV], const double (&Pp)[NV],
-                   const Recip& h, double (&S)[NV]) {
-#pragma unroll
-    for (int n = 0; n < NV; n++) S[n] = h.div(limit<LIM>(P0[n] - Pm[n], Pp[n] - P0[n]));
-  };
-  // y face between rows J and J+1 (src/Main.c:359-365)
-  auto yface = [&](const double (&Pb)[NV], const double (&Sb)[NV], const double (&Pt)[NV],
-                   const double (&St)[NV], int J, double (&G)[NV]) {
-    double lo[NV], hi[NV];
-#pragma unroll
-    for (int n = 0; n < NV; n++) {
-      lo[n] = Pb[n] + hdy * Sb[n];
-      hi[n] = Pt[n] - hdy * St[n];
-    }
-    const double lam = hll<2>(lo, hi, G);
-    if (col_face && J >= 1 && J <= nyp - 3 && lam > lamy) lamy = lam;
-  };
-
-  double P0[NV], P1[NV], P2[NV], S0[NV], S1[NV], Gm[NV];
-  const int J0 = w.J0;
-  {
-    double Pm[NV];
-    if (J0 >= 2) {
-      double Pmm[NV], Sm[NV];
-      prim_at(J0 - 2, Pmm);
-      prim_at(J0 - 1, Pm);
-      prim_at(J0, P0);
-      prim_at(J0 + 1, P1);
-      slope(Pmm, Pm, P0, rdy, Sm);
-      slope(Pm, P0, P1, rdy, S0);
-      if (lane >= 2 && lane <= 29) yface(Pm, Sm, P0, S0, J0 - 1, Gm);
-    } else {
-      prim_at(J0 - 1, Pm);
-      prim_at(J0, P0);
-      prim_at(J0 + 1, P1);
-      slope(Pm, P0, P1, rdy, S0);
-#pragma unroll
-      for (int n = 0; n < NV; n++) Gm[n] = 0.0;
-    }
-  }
-
-  for (int J = J0; J < w.J1; J++) {
-    prim_at(J + 2, P2);
-    slope(P0, P1, P2, rdy, S1);
-    double G[NV];
-    if (lane >= 2 && lane <= 29) yface(P0, S0, P1, S1, J, G);
-
-    // x slope and x face C | C+1 of row J (src/Main.c:346-347, 372-378)
-    double Pl[NV], Pr[NV], Sx[NV], lo[NV], hi[NV], F[NV], Fm[NV];
-    shfl_up9(P0, Pl);
-    shfl_down9(P0, Pr);
-#pragma unroll
-    for (int n = 0; n < NV; n++) {
-      Sx[n] = rdx.div(limit<LIM>(P0[n] - Pl[n], Pr[n] - P0[n]));
-      lo[n] = P0[n] + hdx * Sx[n];
-      Pl[n] = P0[n] - hdx * Sx[n];
-    }
-    shfl_down9(Pl, hi);
-    if (lane >= 1 && lane <= 29) {
-      const double lam = hll<1>(lo, hi, F);
-      if (col_face && J >= 1 && J <= nyp - 3 && lam > lamx) lamx = lam;
-    }
-    shfl_up9(F, Fm);
-
-    // cell update of row J (src/Main.c:323-331, 367-393)
-    if (col_out && J >= NG && J <= nyp - 1 - NG) {
-      const long long idx = (long long)J * pitch + C + 1;
-      double U[NV], Q[NV], R[NV];
-      load_cell(in, plane, idx, U);
+  // The march: iteration r forms the primitives of row r, the y slope of row r-1
+  // and the y face (r-2 | r-1), then finishes row J = r-2 (x face, update).
+  const int rs = w.J0 >= 2 ? w.J0 - 2 : w.J0 - 1;
+  int s0 = rs % 3;                 // window slot of row r
+  for (int r = rs; r <= w.J1 + 1; r++) {
+    const int sm1 = s0 == 0 ? 2 : s0 - 1, sm2 = sm1 == 0 ? 2 : sm1 - 1;
+    // (a) projected primitives of row r: Aux.Prim (src/Main.c:314-336)
+    {
+      double U[NV], Q[NV];
+      const bool ok = col_in && r >= 0 && r < nyp;
+      if (ok) load_cell(in, plane, (long long)r * pitch + C + 1, U);
+      else benign(U);
       primitive(U, Q);
-      relax<2 * HEUN>(Q, R, dt, Kn, Fx);
-      if (HEUN == 1) {
-        double R0[NV];
-        load_cell(d0, plane, idx, U);
-        primitive(U, Q);
-        relax<-1>(Q, R0, dt, Kn, Fx);
-#pragma unroll
-        for (int n = 0; n < NV; n++) R[n] += R0[n];
+      if (ok && col_cell && r >= 1 && r <= nyp - 2) {
+        const double c = relax_cfl<2 * HEUN>(Q, dt, Kn);
+        if (c > prod) prod = c;
       }
+      if (!(col_ring || r == 0 || r == nyp - 1)) {
+        double V[NV];
+        relax<2 * HEUN + 1>(Q, V, dt, Kn, Fx);
+        primitive(V, Q);
+      }
+#pragma unroll
+      for (int n = 0; n < NV; n++) win.P[s0][n][lane] = Q[n];
+    }
+    // (b) y slope of row r-1 (src/Main.c:348-349) and the y face (r-2 | r-1)
+    double G[NV];
+    const bool face_now = r >= rs + 3;
+    if (r >= rs + 2) {
+      double hi[NV];
 #pragma unroll
       for (int n = 0; n < NV; n++) {
-        double v = R[n];
-        v += dtdx * Fm[n];
-        v += dtdy * Gm[n];
-        v -= dtdy * G[n];
-        v -= dtdx * F[n];
-        if (HEUN == 1) v = 0.5 * v;
-        out[n * plane + idx] = v;
+        const double pm = win.P[sm2][n][lane], p0 = win.P[sm1][n][lane], pp = win.P[s0][n][lane];
+        const double S = rdy.div(limit<LIM>(p0 - pm, pp - p0));
+        hi[n] = p0 - hdy * S;
+        G[n] = p0 + hdy * S;                  // lower state of the next face, parked in G
+      }
+      if (face_now && ylane) {
+        double lo[NV];
+#pragma unroll
+        for (int n = 0; n < NV; n++) {
+          lo[n] = win.lo[n][lane];
+          win.lo[n][lane] = G[n];
+        }
+        const double lam = hll<2>(lo, hi, G);
+        const int J = r - 2;
+        if (col_face && J >= 1 && J <= nyp - 3 && lam > lamy) lamy = lam;
+      } else {
+#pragma unroll
+        for (int n = 0; n < NV; n++) win.lo[n][lane] = G[n];
       }
     }
-    copy9(P1, P0);
-    copy9(P2, P1);
-    copy9(S1, S0);
-    copy9(G, Gm);
+    // (c) row J = r-2: x slope, x face C | C+1 (src/Main.c:346-347, 372-378), update
+    const int J = r - 2;
+    if (J >= w.J0 && J < w.J1) {
+      double P0[NV], Sx[NV], lo[NV], hi[NV], F[NV];
+#pragma unroll
+      for (int n = 0; n < NV; n++) {
+        P0[n] = win.P[sm2][n][lane];
+        const double pl = __shfl_up_sync(0xffffffffu, P0[n], 1);
+        const double pr = __shfl_down_sync(0xffffffffu, P0[n], 1);
+        Sx[n] = rdx.div(limit<LIM>(P0[n] - pl, pr - P0[n]));
+        lo[n] = P0[n] + hdx * Sx[n];
+        hi[n] = __shfl_down_sync(0xffffffffu, P0[n] - hdx * Sx[n], 1);
+      }
+#pragma unroll
+      for (int n = 0; n < NV; n++) F[n] = 0.0;
+      if (lane >= 1 && lane <= 29) {
+        const double lam = hll<1>(lo, hi, F);
+        if (col_face && J >= 1 && J <= nyp - 3 && lam > lamx) lamx = lam;
+      }
+      double Fm[NV];
+#pragma unroll
+      for (int n = 0; n < NV; n++) Fm[n] = __shfl_up_sync(0xffffffffu, F[n], 1);
+      // cell update of row J (src/Main.c:323-331, 367-393)
+      if (col_out && J >= NG && J <= nyp - 1 - NG) {
+        const long long idx = (long long)J * pitch + C + 1;
+        double U[NV], Q[NV], R[NV];
+        load_cell(in, plane, idx, U);
+        primitive(U, Q);
+        relax<2 * HEUN>(Q, R, dt, Kn, Fx);
+        if (HEUN == 1) {
+          double R0[NV];
+          load_cell(d0, plane, idx, U);
+          primitive(U, Q);
+          relax<-1>(Q, R0, dt, Kn, Fx);
+#pragma unroll
+          for (int n = 0; n < NV; n++) R[n] += R0[n];
+        }
+#pragma unroll
+        for (int n = 0; n < NV; n++) {
+          double v = R[n];
+          v += dtdx * Fm[n];
+          v += dtdy * win.G[n][lane];
+          v -= dtdy * G[n];
+          v -= dtdx * F[n];
+          if (HEUN == 1) v = 0.5 * v;
+          out[n * plane + idx] = v;
+        }
+      }
+    }
+    if (face_now && ylane) {
+#pragma unroll
+      for (int n = 0; n < NV; n++) win.G[n][lane] = G[n];
+    }
+    s0 = s0 == 2 ? 0 : s0 + 1;
   }
 
   // per-block maxima; the values are >= 0 (or NaN, which never passes a '>' test
@@ -205,12 +197,26 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   }
 }
 
+// Persistent grid (as many CTAs as fit on the SMs); every warp takes the next work
+// item from a counter until the table is exhausted, so uneven blocks and the last
+// wave balance themselves.
 template <int HEUN, int LIM>
-__global__ void __launch_bounds__(128) stage_kernel(const StageArgs a) {
-  const int lane = threadIdx.x & 31;
-  const int warps = blockDim.x >> 5;
-  for (int w = blockIdx.x * warps + (threadIdx.x >> 5); w < a.nwork; w += gridDim.x * warps)
-    stage_item<HEUN, LIM>(a, a.work[w], lane);
+__global__ void __launch_bounds__(32 * STAGE_WARPS, STAGE_MIN_CTAS) stage_kernel(const StageArgs a) {
+  __shared__ WarpWindow win[STAGE_WARPS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    int w = 0;
+    if (lane == 0) w = atomicAdd(a.queue, 1);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (w >= a.nwork) break;
+    stage_item<HEUN, LIM>(a, a.work[w], lane, win[warp]);
+  }
+}
+
+int stage_ctas_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<1, 4>, 32 * STAGE_WARPS, 0);
+  return n > 0 ? n : 1;
 }
 
 // ---------------------------------------------------------------- ghost fill --
@@ -251,8 +257,9 @@ __global__ void ghost_kernel(const BlockDev* __restrict__ blk, const CaseDev* __
 // CFL = max over stages and blocks of dt*lx/dx + dt*ly/dy + prod; reject if
 // CFL > CFLmax, else accept, swap DATA/NEW and advance t; next dt = dt*CFLreg/CFL.
 __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __restrict__ blk,
-                               unsigned long long* lam, double* trace, cudaGraphConditionalHandle h,
-                               int use_handle) {
+                               unsigned long long* lam, double* trace, int* queues,
+                               cudaGraphConditionalHandle h, int use_handle) {
+  if (threadIdx.x < 2) queues[threadIdx.x] = 0;   // both stages' work counters
   int live = 0;
   for (int c = threadIdx.x; c < ncases; c += blockDim.x) {
     CaseDev& cs = cases[c];
@@ -317,6 +324,20 @@ __global__ void stage_cfl_kernel(const BlockDev* __restrict__ blk, int nblk, con
   s[0] = s[1] = s[2] = 0ull;
 }
 
+// uniform state at rest (rho = theta = 1) in every cell of a block, for tuning runs
+__global__ void fill_block_uniform(double* __restrict__ base, long long plane) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= plane) return;
+  const double v[NV] = {1.0, 0.0, 0.0, 1.5, 1.0, 0.0, 1.0, 0.0, 0.0};
+#pragma unroll
+  for (int m = 0; m < NV; m++) base[m * plane + k] = v[m];
+}
+
+cudaError_t launch_fill_uniform(double* base, long long plane, cudaStream_t s) {
+  fill_block_uniform<<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(base, plane);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ transposes --
 // host layout (cells x 9, x fastest, ghosts included) <-> device planes
 __global__ void aos_to_planes(const double* __restrict__ aos, double* __restrict__ dst, int nxp,
@@ -345,11 +366,11 @@ __global__ void planes_to_aos(const double* __restrict__ src, double* __restrict
 template <int HEUN>
 static cudaError_t launch_stage_lim(int lim, const StageArgs& a, int grid, cudaStream_t s) {
   switch (lim) {
-    case 0: stage_kernel<HEUN, 0><<<grid, 128, 0, s>>>(a); break;
-    case 1: stage_kernel<HEUN, 1><<<grid, 128, 0, s>>>(a); break;
-    case 2: stage_kernel<HEUN, 2><<<grid, 128, 0, s>>>(a); break;
-    case 3: stage_kernel<HEUN, 3><<<grid, 128, 0, s>>>(a); break;
-    default: stage_kernel<HEUN, 4><<<grid, 128, 0, s>>>(a); break;
+    case 0: stage_kernel<HEUN, 0><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
+    case 1: stage_kernel<HEUN, 1><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
+    case 2: stage_kernel<HEUN, 2><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
+    case 3: stage_kernel<HEUN, 3><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
+    default: stage_kernel<HEUN, 4><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
   }
   return cudaGetLastError();
 }
@@ -367,9 +388,9 @@ cudaError_t launch_ghost(const BlockDev* blk, const CaseDev* cases, const GhostE
 }
 
 cudaError_t launch_control(CaseDev* cases, int ncases, const BlockDev* blk, unsigned long long* lam,
-                           double* trace, cudaGraphConditionalHandle h, int use_handle,
+                           double* trace, int* queues, cudaGraphConditionalHandle h, int use_handle,
                            cudaStream_t s) {
-  control_kernel<<<1, 256, 0, s>>>(cases, ncases, blk, lam, trace, h, use_handle);
+  control_kernel<<<1, 256, 0, s>>>(cases, ncases, blk, lam, trace, queues, h, use_handle);
   return cudaGetLastError();
 }
 

@@ -41,8 +41,16 @@ __device__ __forceinline__ bool div_range_ok(double y) {
 struct Recip {        // 1/y for a denominator shared by several quotients
   double y, r;
   bool ok;
-  __device__ __forceinline__ explicit Recip(double y_) : y(y_), r(__drcp_rn(y_)), ok(div_range_ok(y_)) {}
-  __device__ __forceinline__ Recip(double y_, double r_) : y(y_), r(r_), ok(true) {}
+  __device__ __forceinline__ explicit Recip(double y_) {
+    y = y_;
+    r = __drcp_rn(y_);
+    ok = div_range_ok(y_);
+  }
+  __device__ __forceinline__ Recip(double y_, double r_) {   // r_ = RN(1/y_), y_ in range
+    y = y_;
+    r = r_;
+    ok = true;
+  }
   __device__ __forceinline__ double div(double x) const {
     const long long bx = __double_as_longlong(x);
     if (ok && ((unsigned)(bx >> 52) & 0x7ffu) - 543u <= 960u) {

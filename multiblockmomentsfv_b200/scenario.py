@@ -109,10 +109,20 @@ def initial_state(s: Scenario, x, y, t: float = 0.0) -> np.ndarray:
 
 def initial_block(s: Scenario, b: Block) -> np.ndarray:
     """Interior of L_DATA set from the scenario, ghosts zero (src/Main.c:113-136).
-    Returns (nyp, nxp, 9), x fastest."""
+    Returns (nyp, nxp, 9), x fastest.  Piecewise-constant states are evaluated once
+    per state and scattered (the same bits as evaluating every cell)."""
     U = np.zeros((b.nyp, b.nxp, NV))
     x, y = b.centres()
     inner = (slice(NG, b.nyp - NG), slice(NG, b.nxp - NG))
+    if s.kind in (KIND_QUADRANT, KIND_UNIFORM):
+        st = np.asarray(s.states, dtype=np.float64)
+        table = moments(st[:, 0], st[:, 1], st[:, 2], st[:, 3])          # (4, 9)
+        if s.kind == KIND_UNIFORM:
+            U[inner] = table[0]
+        else:
+            k = (x[inner] >= 0.0).astype(np.int64) + 2 * (y[inner] >= 0.0).astype(np.int64)
+            U[inner] = table[k]
+        return U
     U[inner] = initial_state(s, x[inner], y[inner], 0.0)
     return U
 

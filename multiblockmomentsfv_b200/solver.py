@@ -137,6 +137,12 @@ class Solver:
         self._check(self.L.mbm_attempts(self.ctx, C.byref(a)))
         return a.value
 
+    def config(self) -> dict:
+        """Launch configuration: rows per work item, work items, persistent CTAs."""
+        a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
+        self._check(self.L.mbm_config(self.ctx, C.byref(a), C.byref(b), C.byref(c)))
+        return {"segment_rows": a.value, "work_items": b.value, "ctas": c.value}
+
     def time_stage(self, heun: int, dt: float, reps: int = 10) -> float:
         """Mean device milliseconds of one stage-kernel launch (CUDA events)."""
         ms = C.c_double(0.0)
@@ -149,6 +155,130 @@ class Solver:
         n = C.c_int(0)
         self._check(self.L.mbm_trace(self.ctx, _dptr(buf), cap, C.byref(n)))
         return buf[:n.value].copy()
+
+
+class BatchSolver:
+    """Many independent cases (each a deck with its own blocks, Kn, F and limiter) in
+    one device context, advanced together by one CUDA-graph loop with per-case dt."""
+
+    def __init__(self, cases, device: int = 0, show_every: int = 0, stream: Optional[int] = None,
+                 segment_rows: int = 0, max_attempts: int = 0):
+        """cases: list of (Deck, Scenario or None)."""
+        self.cases = list(cases)
+        self.L = _abi.lib()
+        blocks, descs = [], (_abi.CaseDesc * len(self.cases))()
+        self.first = []
+        for k, (d, _) in enumerate(self.cases):
+            descs[k].first_block = len(blocks)
+            descs[k].nblocks = len(d.blocks)
+            descs[k].Kn, descs[k].F, descs[k].limiter = d.Kn, d.F, d.limiter
+            self.first.append(len(blocks))
+            blocks.extend(d.blocks)
+        self.blocks = blocks
+        self._bd = _abi.block_descs(blocks)
+        self._cd = descs
+        p = _abi.Params()
+        p.mode, p.device, p.show_every, p.max_attempts, p.segment_rows = (_abi.MODE_EXACT, device,
+                                                                          show_every, max_attempts, segment_rows)
+        p.stream = stream
+        p.Kn, p.limiter = self.cases[0][0].Kn, self.cases[0][0].limiter
+        self._params = p
+        ctx = C.c_void_p()
+        st = self.L.mbm_create_batch(self._bd, len(blocks), descs, len(self.cases), C.byref(p), C.byref(ctx))
+        if st != _abi.MBM_OK:
+            raise _abi.MBMError(st, self.L.mbm_last_error(None).decode())
+        self.ctx = ctx
+        for k, (d, scn) in enumerate(self.cases):
+            if scn is None:
+                continue
+            for b, blk in enumerate(d.blocks):
+                for side in range(4):
+                    if blk.bc[side] <= -2:
+                        v = np.ascontiguousarray(sc.dirichlet_edge(scn, blk, side, 0.0))
+                        _abi.check(self.L.mbm_set_dirichlet(self.ctx, self.first[k] + b, side, _dptr(v)), self.ctx)
+
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.L.mbm_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, layer: int, k: int, b: int, U: np.ndarray) -> None:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        _abi.check(self.L.mbm_upload(self.ctx, layer, self.first[k] + b, _dptr(U)), self.ctx)
+
+    def download(self, layer: int, k: int, b: int) -> np.ndarray:
+        blk = self.cases[k][0].blocks[b]
+        U = np.empty((blk.nyp, blk.nxp, bf.NV))
+        _abi.check(self.L.mbm_download(self.ctx, layer, self.first[k] + b, _dptr(U)), self.ctx)
+        return U
+
+    def initialise(self) -> None:
+        for k, (d, scn) in enumerate(self.cases):
+            for b, blk in enumerate(d.blocks):
+                self.upload(L_DATA, k, b, sc.initial_block(scn, blk))
+        _abi.check(self.L.mbm_set_boundary(self.ctx, L_DATA, 0.0), self.ctx)
+
+    def steps(self, t, tend, max_steps: int = 0, CFLmax: float = 1.0, CFLreg: float = 0.95):
+        """Advance every case; returns (t[], nsteps[], nrej[])."""
+        n = len(self.cases)
+        tt = np.ascontiguousarray(np.broadcast_to(np.asarray(t, dtype=np.float64), (n,)).copy())
+        te = np.ascontiguousarray(np.broadcast_to(np.asarray(tend, dtype=np.float64), (n,)).copy())
+        ns = (C.c_int * n)()
+        nr = (C.c_int * n)()
+        _abi.check(self.L.mbm_steps_batch(self.ctx, _dptr(tt), _dptr(te), CFLmax, CFLreg, max_steps, ns, nr),
+                   self.ctx)
+        return tt, np.array(ns[:]), np.array(nr[:])
+
+    def attempts(self) -> int:
+        a = C.c_int(0)
+        _abi.check(self.L.mbm_attempts(self.ctx, C.byref(a)), self.ctx)
+        return a.value
+
+
+def batch_workload(seed: int, ncases: int = 64, nmin: int = 64, nmax: int = 1024):
+    """The many-case workload: seeded cases of 1-4 blocks tiling [-1,1]^2 (one block,
+    two or three strips, or a 2 x 2 tiling; conforming interfaces), n in [nmin, nmax]
+    cells per block side, Kn log-uniform in [1e-3, 1e-1], R13 in {0, 1}, limiter
+    uniform over the five, seeded quadrant initial state, open outer edges.
+    Returns a list of (Deck, Scenario)."""
+    rng = np.random.default_rng(seed)
+    out_cases = []
+    for k in range(ncases):
+        nb = int(rng.integers(1, 5))
+        n = int(rng.integers(nmin, nmax + 1))
+        B = bf.Block
+        if nb == 1:
+            blocks = [B(1, -1.0, 1.0, -1.0, 1.0, n, n, (0, 0, 0, 0))]
+        elif nb == 2:
+            blocks = [B(1, -1.0, 0.0, -1.0, 1.0, n, n, (0, 2, 0, 0)),
+                      B(2, 0.0, 1.0, -1.0, 1.0, n, n, (1, 0, 0, 0))]
+        elif nb == 3:
+            h = 2.0 / 3.0
+            blocks = [B(1, -1.0, 1.0, -1.0, -1.0 + h, n, n, (0, 0, 0, 2)),
+                      B(2, -1.0, 1.0, -1.0 + h, -1.0 + 2 * h, n, n, (0, 0, 1, 3)),
+                      B(3, -1.0, 1.0, -1.0 + 2 * h, 1.0, n, n, (0, 0, 2, 0))]
+        else:
+            blocks = [B(1, -1.0, 0.0, -1.0, 0.0, n, n, (0, 2, 0, 3)),
+                      B(2, 0.0, 1.0, -1.0, 0.0, n, n, (1, 0, 0, 4)),
+                      B(3, -1.0, 0.0, 0.0, 1.0, n, n, (0, 4, 1, 0)),
+                      B(4, 0.0, 1.0, 0.0, 1.0, n, n, (3, 0, 2, 0))]
+        d = bf.Deck(Kn=float(10 ** rng.uniform(-3, -1)), R13=float(rng.integers(0, 2)),
+                    limiter=int(rng.integers(0, 5)), CFL=0.95)
+        d.blocks = blocks
+        out_cases.append((d, sc.Scenario.seeded_quadrant(seed * 1000 + k)))
+    return out_cases
 
 
 def ghost_map(blocks: Sequence[bf.Block]) -> np.ndarray:
