@@ -259,7 +259,7 @@ __global__ void ghost_kernel(const BlockDev* __restrict__ blk, const CaseDev* __
 __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __restrict__ blk,
                                unsigned long long* lam, double* trace, int* queues,
                                cudaGraphConditionalHandle h, int use_handle) {
-  if (threadIdx.x < 2) queues[threadIdx.x] = 0;   // both stages' work counters
+  if (threadIdx.x < 10) queues[threadIdx.x] = 0;  // work counters [stage][limiter]
   int live = 0;
   for (int c = threadIdx.x; c < ncases; c += blockDim.x) {
     CaseDev& cs = cases[c];
