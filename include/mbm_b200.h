@@ -157,6 +157,36 @@ int mbm_config(mbm_ctx *ctx, int *segment_rows, int *work_items, int *ctas);
  * src < 0 is Dirichlet row -(src+1), flags bit 0/1 = x/y wall sign.  Needs no GPU. */
 int mbm_ghost_map(const mbm_block_desc *blocks, int nblocks, int *entries, int cap, int *n);
 
+/* One Heun stage -- Update (src/Main.c:297-396) of every block -- on device buffers
+ * the caller owns, allocating no device memory: no cudaMalloc, cudaFree or
+ * allocating library routine is called.  No counterpart in the reference (its
+ * Update allocates nothing on a GPU because it has none); it exists for callers
+ * that cannot allocate: a framework whose memory pool owns the GPU, code running
+ * inside CUDA-graph capture, loops that fix every allocation at start-up.
+ *
+ * in, data0 and out are device arrays in this library's plane layout: blocks one
+ * after another; block b has 9 planes (one per moment) of (ny+6) rows x pitch
+ * doubles, pitch = ((nx+6) + 1 + 3) & ~3, plane = (pitch*(ny+6) + 31) & ~31
+ * elements, moment m of padded cell (I, J) at offset_b + m*plane + J*pitch + I + 1,
+ * offset_0 = 0, offset_{b+1} = offset_b + 9*plane_b.  Stage 1 (heun 0) reads `in`
+ * (DATA with filled ghosts); stage 2 (heun 1) reads `in` (TMP) and `data0` (DATA).
+ * Interior cells of `out` are written; its ghost cells are left as they are (fill
+ * them with SetBoundary semantics before the next stage).  Sync codes are ignored
+ * here.  cfl[b] (host, may be NULL) receives each block's Update return value.
+ * Launches on `stream` (a cudaStream_t, NULL = the legacy default stream) and
+ * waits for it.
+ *
+ * Scratch: one file-scope device array of 320 KB (held by every GPU that loads
+ * the library until the process exits): at most 64 blocks and 19,968 warp work
+ * items (28-column strips x 32-row segments, e.g. 16 blocks of 1024^2); larger
+ * inputs return MBM_EINVAL.  Its device address is looked up on the first call on
+ * each device -- make that first call before any stream capture.  Every call
+ * shares the array and clears what must start at zero; calls that overlap on the
+ * GPU race.  Errors: mbm_last_error(NULL). */
+int mbm_stage_noalloc(const mbm_block_desc *blocks, int nblocks, const double *in,
+                      const double *data0, double *out, double Kn, double F, int limiter,
+                      double dt, int heun, double *cfl, void *stream);
+
 const char *mbm_strerror(int status);
 /* last CUDA / validation message of a context (or the last mbm_create failure when ctx is NULL) */
 const char *mbm_last_error(mbm_ctx *ctx);

@@ -19,7 +19,7 @@ EXPORTS = (
     "mbm_create", "mbm_destroy", "mbm_upload", "mbm_download", "mbm_set_dirichlet",
     "mbm_set_boundary", "mbm_update", "mbm_time_update", "mbm_steps", "mbm_steps_capped",
     "mbm_time_stage", "mbm_trace", "mbm_attempts", "mbm_config",
-    "mbm_create_batch", "mbm_steps_batch", "mbm_trace_case",
+    "mbm_create_batch", "mbm_steps_batch", "mbm_trace_case", "mbm_stage_noalloc",
     "mbm_ghost_map", "mbm_strerror", "mbm_last_error", "mbm_version",
 )
 
@@ -50,12 +50,13 @@ _lib = None
 
 
 def lib(path: str = None):
-    """Load the library (building it first if it is missing or stale)."""
+    """Load the library (building it first if it is missing).  MBM_LIBRARY may name
+    another build of it (e.g. a variant under test)."""
     global _lib
     if _lib is not None:
         return _lib
     if path is None:
-        path = _build.LIB
+        path = os.environ.get("MBM_LIBRARY") or _build.LIB
         if not os.path.exists(path):
             _build.build()
     L = C.CDLL(path)
@@ -80,6 +81,8 @@ def lib(path: str = None):
     L.mbm_create_batch.argtypes = [P(BlockDesc), C.c_int, P(CaseDesc), C.c_int, P(Params), P(vp)]
     L.mbm_steps_batch.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_int, P(C.c_int), P(C.c_int)]
     L.mbm_trace_case.argtypes = [vp, C.c_int, dp, C.c_int, P(C.c_int)]
+    L.mbm_stage_noalloc.argtypes = [P(BlockDesc), C.c_int, vp, vp, vp, C.c_double, C.c_double, C.c_int,
+                                    C.c_double, C.c_int, dp, vp]
     L.mbm_ghost_map.argtypes = [P(BlockDesc), C.c_int, P(C.c_int), C.c_int, P(C.c_int)]
     L.mbm_strerror.restype = C.c_char_p
     L.mbm_strerror.argtypes = [C.c_int]

@@ -14,7 +14,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libmbm_b200.so")
 
-SOURCES = ["mbm_host.cu", "mbm_kernels.cu"]
+SOURCES = ["mbm_host.cu", "mbm_kernels.cu", "mbm_noalloc.cu"]
 HEADERS = ["mbm_internal.h", "mbm_math.cuh"]
 
 NVCC_FLAGS = [

@@ -39,6 +39,10 @@ using namespace mbm;
 
 static thread_local std::string g_create_error;
 
+namespace mbm {
+void set_global_error(const std::string& msg) { g_create_error = msg; }
+}  // namespace mbm
+
 struct LimGroup {      // the work items of every block whose case uses one limiter
   int lim, start, count, grid;
 };
