@@ -43,10 +43,9 @@ def measured_peaks():
 
 
 def workload(n, seed):
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import helpers as H
+    from multiblockmomentsfv_b200 import blockfile as bf
     from multiblockmomentsfv_b200 import scenario as sc
-    d = H.quadrant_deck(n, Kn=0.01, R13=1.0)
+    d = bf.quadrant_deck(n, Kn=0.01, R13=1.0)
     return d, sc.Scenario.seeded_quadrant(seed)
 
 
@@ -144,7 +143,10 @@ def batched_leg(a, local, stream, rank):
     """Many independent cases: one context advancing all of them in one CUDA-graph
     loop (per-case dt, one persistent launch per limiter per stage) against the same
     cases run one after another, each in its own context.  Device time (CUDA events)
-    of the step loops only; context creation and initial states are outside."""
+    of the step loops only; context creation and initial states are outside.  A case
+    that produces a non-finite value stops there in both arms (the unlimited
+    'average' slopes blow up on some quadrant states, in the reference too); the
+    throughput counts the steps each case took."""
     import torch
     from multiblockmomentsfv_b200 import solver as sv
     cases = sv.batch_workload(seed=a.seed + rank, ncases=a.batch_cases)
@@ -152,34 +154,66 @@ def batched_leg(a, local, stream, rank):
     ev = lambda: torch.cuda.Event(enable_timing=True)
     with sv.BatchSolver(cases, device=local, stream=stream.cuda_stream) as bs:
         bs.initialise()
-        bs.steps(0.0, 10.0, max_steps=2)
+        bs.steps(0.0, 10.0, max_steps=2, check=False)
+        bs.initialise()
         e0, e1 = ev(), ev()
         e0.record(stream)
-        _, ns, _ = bs.steps(0.0, 10.0, max_steps=a.batch_steps)
+        _, ns, _ = bs.steps(0.0, 10.0, max_steps=a.batch_steps, check=False)
         e1.record(stream)
         stream.synchronize()
         ms_b = e0.elapsed_time(e1)
         launches = bs.attempts()
+        status = bs.case_status()
     upd_b = float(sum(c * n for c, n in zip(cells, ns)))
-    ms_s, upd_s = 0.0, 0.0
+    ms_s, upd_s, ns_serial = 0.0, 0.0, []
     for (d, scn), c in zip(cases, cells):
-        with sv.Solver(d, scn, device=local, show_every=0, stream=stream.cuda_stream) as s1:
+        with sv.BatchSolver([(d, scn)], device=local, stream=stream.cuda_stream) as s1:
             s1.initialise()
-            s1.steps(0.0, 10.0, max_steps=2)
+            s1.steps(0.0, 10.0, max_steps=2, check=False)
+            s1.initialise()
             e0, e1 = ev(), ev()
             e0.record(stream)
-            _, n1, _ = s1.steps(0.0, 10.0, max_steps=a.batch_steps)
+            _, n1, _ = s1.steps(0.0, 10.0, max_steps=a.batch_steps, check=False)
             e1.record(stream)
             stream.synchronize()
             ms_s += e0.elapsed_time(e1)
-            upd_s += c * n1
+            upd_s += c * int(n1[0])
+            ns_serial.append(int(n1[0]))
+    failed = [{"case": k, "limiter": cases[k][0].limiter, "steps": int(ns[k])}
+              for k in range(len(cases)) if status[k] != 0]
     return {"cases": len(cases), "steps_per_case": a.batch_steps, "cells": int(sum(cells)),
             "value": upd_b / (ms_b / 1e3), "serial_value": upd_s / (ms_s / 1e3),
             "ratio": (upd_b / ms_b) / (upd_s / ms_s), "unit": "cell-updates/s",
             "ms": ms_b, "serial_ms": ms_s, "graph_attempts": launches,
-            "workload": "64 seeded cases, 1-4 blocks of n x n, n ~ U{64..1024}, Kn log-U[1e-3,1e-1], "
-                        "R13 in {0,1}, limiter ~ U{5}, quadrant state, open edges, 200 steps each, "
-                        "per-case dt; serial = the same cases one context and one Steps loop each"}
+            "same_steps_as_serial": [int(x) for x in ns] == ns_serial,
+            "stopped_nonfinite": failed,
+            "workload": f"{len(cases)} seeded cases, 1-4 blocks of n x n, n ~ U{{64..1024}}, Kn log-U[1e-3,1e-1], "
+                        "R13 in {0,1}, limiter ~ U{5}, quadrant state, open edges, "
+                        f"{a.batch_steps} steps each, per-case dt; serial = the same cases one context and one "
+                        "Steps loop each"}
+
+
+def adjoint_leg(a, local, stream):
+    """The discrete adjoint: J = sum(qx^2 + qy^2) after N Heun steps on 4 blocks of
+    n x n cells, gradient wrt the initial temperature field and Kn, checkpoints every
+    k steps.  Device times of the forward run (with checkpoints and the dt record)
+    and of the reverse sweep (segment recomputation included), from mbm_adjoint_run."""
+    import numpy as np
+    from multiblockmomentsfv_b200 import adjoint as adj
+    from multiblockmomentsfv_b200 import blockfile as bf
+    n, nsteps, every = a.adjoint_n, a.adjoint_steps, a.adjoint_every
+    d = bf.quadrant_deck(n, Kn=0.01)
+    base = adj.smooth_base(d, a.seed)
+    th0 = [np.ones((b.ny, b.nx)) for b in d.blocks]
+    with adj.Sensitivity(d, base, device=local, stream=stream.cuda_stream) as S:
+        layers = adj.state_from_theta(d, base, th0)
+        S.load(layers)
+        S.run(min(nsteps, 2 * every), every)          # warm-up
+        S.load(layers)
+        J, g, gK, dts, ms = S.run(nsteps, every)
+    return {"case": f"4 blocks x {n}^2, {nsteps} Heun steps, checkpoints every {every}, "
+                    "J = sum(qx^2+qy^2) of the final state, grad wrt theta0 field and Kn, dt frozen",
+            "forward_ms": ms[0], "adjoint_ms": ms[1], "ratio": ms[1] / ms[0], "J": J, "dJ_dKn": gK}
 
 
 def main():
@@ -196,6 +230,9 @@ def main():
     ap.add_argument("--segment-rows", type=int, default=0)
     ap.add_argument("--batch-cases", type=int, default=64, help="cases in the batched-vs-serial leg (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--adjoint-n", type=int, default=256, help="cells per block side in the adjoint leg (0 = skip)")
+    ap.add_argument("--adjoint-steps", type=int, default=200)
+    ap.add_argument("--adjoint-every", type=int, default=20)
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3
@@ -298,6 +335,7 @@ def main():
 
     s.close()
     batched = batched_leg(a, local, stream, rank) if a.batch_cases > 0 else None
+    adjoint = adjoint_leg(a, local, stream) if a.adjoint_n > 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -335,6 +373,7 @@ def main():
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "batched": batched,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -49,13 +49,13 @@ extern "C" {
 typedef struct {
   int nx, ny;          /* interior cells; the block holds (nx+6)*(ny+6) cells       */
   double x0, y0;       /* centre of padded cell (0,0): B.x, B.y (src/Mesh.c:364-365) */
-  double dx, dy;
+  double dx, dy;       /* cell sizes, in (1e-100, 1e100)                           */
   int bc[4];           /* left, right, bottom, top: >0 sync with block code,
                           0 open, -1 wall, -2 Dirichlet (src/defs.h:26-31)          */
 } mbm_block_desc;
 
 typedef struct {
-  double Kn;           /* Knudsen number (collision frequency rho*sqrt(theta)/Kn)   */
+  double Kn;           /* Knudsen number (collision frequency rho*sqrt(theta)/Kn), in (1e-100, 1e100) */
   double F;            /* body force in x                                          */
   int limiter;         /* MBM_LIM_*                                                */
   int mode;            /* MBM_MODE_*                                               */
@@ -64,6 +64,7 @@ typedef struct {
   int max_attempts;    /* bound on step attempts per mbm_steps call; 0 = 10,000,000 */
   int segment_rows;    /* rows per warp work item; 0 = tuned default               */
   void *stream;        /* cudaStream_t to launch on; NULL = a stream the context owns */
+  int adjoint;         /* 1: the step loop records dt and checkpoints for mbm_adjoint_run */
 } mbm_params;
 
 /* One independent case of a batch: a contiguous run of blocks of the block array,
@@ -99,6 +100,12 @@ int mbm_steps_batch(mbm_ctx *ctx, double *t, const double *tend, double CFLmax, 
  * doubles, the reference's CVector layer, src/defs.h:42-44) and the device. */
 int mbm_upload(mbm_ctx *ctx, int layer, int block, const double *cells);
 int mbm_download(mbm_ctx *ctx, int layer, int block, double *cells);
+
+/* Output's payload of one block of DATA computed on the device (src/Output.c:195-243):
+ * the fields rho vx vy T p Pxx Pxy Pyy qx qy over the interior plus one ghost ring,
+ * x outer, y inner, variables fastest; (nx+2)*(ny+2)*10 floats (single = 1) or
+ * doubles, the bytes the reference writes to its .dat file. */
+int mbm_output_fields(mbm_ctx *ctx, int block, int single, void *out);
 
 /* Dirichlet ghost values of one edge (code -2), in FillEdge's order: tangential
  * index over the full edge, corners included, outer; ghost layer n = 1..3 inner
@@ -147,6 +154,13 @@ int mbm_trace_case(mbm_ctx *ctx, int c, double *records, int cap, int *n);
  * runs five kernels (two stages, two ghost fills, the controller). */
 int mbm_attempts(mbm_ctx *ctx, int *attempts);
 
+/* Status of each of the first n cases after the last step-loop call: MBM_OK, or
+ * MBM_ENONFINITE (the case stopped at the attempt that produced a NaN or infinity;
+ * its state is the last accepted one) or MBM_ESTEPLIMIT.  The call itself returned
+ * the worst of them; the other cases ran to the end.  No counterpart in the
+ * reference, whose loop runs on through non-finite values. */
+int mbm_case_status(mbm_ctx *ctx, int *status, int n);
+
 /* Launch configuration in use: rows per warp work item (picked by the autotuner
  * when mbm_params.segment_rows is 0), work items per stage, CTAs of the persistent
  * stage grid. */
@@ -186,6 +200,28 @@ int mbm_ghost_map(const mbm_block_desc *blocks, int nblocks, int *entries, int c
 int mbm_stage_noalloc(const mbm_block_desc *blocks, int nblocks, const double *in,
                       const double *data0, double *out, double Kn, double F, int limiter,
                       double dt, int heun, double *cfl, void *stream);
+
+/* Discrete adjoint (no counterpart in the reference): from the current DATA (the
+ * initial state u0), run Steps for `nsteps` accepted steps (dt restarts at 1e-4,
+ * CFLmax 1, CFLreg as given) recording every dt and a checkpoint every `every`
+ * steps; evaluate J = sum over interior cells of qx^2 + qy^2 of the final state;
+ * then sweep back through the steps with dt frozen, recomputing each segment from
+ * its checkpoint, through the hand-written reverse of Update (relaxation, HLL
+ * fluxes, limiters with one-sided derivatives at kinks) and of SetBoundary.
+ * grad (host, may be NULL) receives dJ/du0 in the layer layout of mbm_upload
+ * (ghost cells zero), *grad_Kn = dJ/dKn, dts[nsteps] (may be NULL) the frozen dt
+ * sequence, ms[0..1] (may be NULL) the forward and the adjoint device times.  *t
+ * advances to the forward run's end.  Needs a single-case context created with
+ * mbm_params.adjoint = 1. */
+int mbm_adjoint_run(mbm_ctx *ctx, double *t, int nsteps, int every, double CFLreg, double *J,
+                    double *grad, double *grad_Kn, double *dts, double *ms);
+
+/* Frozen-dt forward: n Heun steps of DATA with the given dt values (no controller,
+ * as the adjoint sees the run); *J (may be NULL) = the heat-flux functional above. */
+int mbm_replay(mbm_ctx *ctx, const double *dts, int n, double *J);
+
+/* Kn and body force F of every case (the reference's globals Kn, F). */
+int mbm_set_physics(mbm_ctx *ctx, double Kn, double F);
 
 const char *mbm_strerror(int status);
 /* last CUDA / validation message of a context (or the last mbm_create failure when ctx is NULL) */

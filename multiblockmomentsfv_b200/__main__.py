@@ -93,7 +93,7 @@ def main(argv=None) -> int:
             s.set_boundary(sv.L_DATA, 0.0)
         else:
             s.initialise()
-        w.write(s.layers(), 0.0, -1)
+        w.write_solver(s, 0.0, -1)
         t, nmax = 0.0, 0
         for tn in deck.t_out:
             t0 = time.perf_counter()
@@ -104,7 +104,7 @@ def main(argv=None) -> int:
             print("   %d steps (%d rejected) to t = %g, %.4f us per cell-update" %
                   (n, rej, t, el * 1e6 / max(1, deck.full_grid_size * (n + rej))))
             nmax += n
-            w.write(s.layers(), t, nmax)
+            w.write_solver(s, t, nmax)
     print("\n Done after %d steps.\n" % nmax)
     return 0
 

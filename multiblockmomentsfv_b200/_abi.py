@@ -18,8 +18,9 @@ MODE_EXACT = 0
 EXPORTS = (
     "mbm_create", "mbm_destroy", "mbm_upload", "mbm_download", "mbm_set_dirichlet",
     "mbm_set_boundary", "mbm_update", "mbm_time_update", "mbm_steps", "mbm_steps_capped",
-    "mbm_time_stage", "mbm_trace", "mbm_attempts", "mbm_config",
+    "mbm_time_stage", "mbm_trace", "mbm_attempts", "mbm_case_status", "mbm_config",
     "mbm_create_batch", "mbm_steps_batch", "mbm_trace_case", "mbm_stage_noalloc",
+    "mbm_adjoint_run", "mbm_replay", "mbm_set_physics", "mbm_output_fields",
     "mbm_ghost_map", "mbm_strerror", "mbm_last_error", "mbm_version",
 )
 
@@ -32,7 +33,7 @@ class BlockDesc(C.Structure):
 class Params(C.Structure):
     _fields_ = [("Kn", C.c_double), ("F", C.c_double), ("limiter", C.c_int), ("mode", C.c_int),
                 ("device", C.c_int), ("show_every", C.c_int), ("max_attempts", C.c_int),
-                ("segment_rows", C.c_int), ("stream", C.c_void_p)]
+                ("segment_rows", C.c_int), ("stream", C.c_void_p), ("adjoint", C.c_int)]
 
 
 class CaseDesc(C.Structure):
@@ -77,10 +78,15 @@ def lib(path: str = None):
     L.mbm_time_stage.argtypes = [vp, C.c_int, C.c_double, C.c_int, dp]
     L.mbm_trace.argtypes = [vp, dp, C.c_int, P(C.c_int)]
     L.mbm_attempts.argtypes = [vp, P(C.c_int)]
+    L.mbm_case_status.argtypes = [vp, P(C.c_int), C.c_int]
     L.mbm_config.argtypes = [vp, P(C.c_int), P(C.c_int), P(C.c_int)]
     L.mbm_create_batch.argtypes = [P(BlockDesc), C.c_int, P(CaseDesc), C.c_int, P(Params), P(vp)]
     L.mbm_steps_batch.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_int, P(C.c_int), P(C.c_int)]
     L.mbm_trace_case.argtypes = [vp, C.c_int, dp, C.c_int, P(C.c_int)]
+    L.mbm_adjoint_run.argtypes = [vp, dp, C.c_int, C.c_int, C.c_double, dp, dp, dp, dp, dp]
+    L.mbm_replay.argtypes = [vp, dp, C.c_int, dp]
+    L.mbm_set_physics.argtypes = [vp, C.c_double, C.c_double]
+    L.mbm_output_fields.argtypes = [vp, C.c_int, C.c_int, vp]
     L.mbm_stage_noalloc.argtypes = [P(BlockDesc), C.c_int, vp, vp, vp, C.c_double, C.c_double, C.c_int,
                                     C.c_double, C.c_int, dp, vp]
     L.mbm_ghost_map.argtypes = [P(BlockDesc), C.c_int, P(C.c_int), C.c_int, P(C.c_int)]

@@ -250,3 +250,24 @@ def format_deck(d: Deck, title: str = "generated deck") -> str:
         out.append(f"{b.block_id}/{b.xmin!r},{b.xmax!r}/{b.ymin!r},{b.ymax!r}/{nx},{ny}/"
                    f"{b.bc[0]},{b.bc[1]},{b.bc[2]},{b.bc[3]}/")
     return "\n".join(out) + "\n"
+
+
+def quadrant_deck(n: int, Kn: float = 0.01, limiter: int = LIM_HARMONIC, R13: float = 1.0,
+                  nblocks_side: int = 2) -> "Deck":
+    """The scaled square4 layout: blocks of n x n cells tiling [-1,1]^2, all outer
+    edges open (extrapolation), inner edges synchronised."""
+    k = nblocks_side
+    h = 2.0 / k
+    blocks = []
+    for j in range(k):
+        for i in range(k):
+            bid = j * k + i + 1
+            left = bid - 1 if i > 0 else 0
+            right = bid + 1 if i < k - 1 else 0
+            bottom = bid - k if j > 0 else 0
+            top = bid + k if j < k - 1 else 0
+            blocks.append(Block(bid, -1.0 + i * h, -1.0 + (i + 1) * h, -1.0 + j * h,
+                                -1.0 + (j + 1) * h, n, n, (left, right, bottom, top)))
+    d = Deck(Kn=Kn, R13=R13, limiter=limiter, CFL=0.95)
+    d.blocks = blocks
+    return d

@@ -1,7 +1,9 @@
 """Compile the CUDA library in place: multiblockmomentsfv_b200/lib/libmbm_b200.so.
 
-sm_100a only.  -fmad=false keeps every multiply and add separately rounded
-(the bitwise mode depends on it); double division and sqrt are IEEE by default.
+sm_100a only.  -fmad=false keeps every multiply and add of the forward path
+separately rounded (the bitwise mode depends on it); double division and sqrt are
+IEEE by default.  The adjoint kernels are derivatives, not restatements of the
+reference's arithmetic, and are compiled with fused multiply-adds.
 """
 from __future__ import annotations
 
@@ -14,14 +16,15 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libmbm_b200.so")
 
-SOURCES = ["mbm_host.cu", "mbm_kernels.cu", "mbm_noalloc.cu"]
-HEADERS = ["mbm_internal.h", "mbm_math.cuh"]
+SOURCES = ["mbm_host.cu", "mbm_kernels.cu", "mbm_noalloc.cu", "mbm_adjoint.cu"]
+HEADERS = ["mbm_internal.h", "mbm_math.cuh", "mbm_adjoint_math.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-lineinfo", "-O3", "-fmad=false", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-lineinfo", "-O3", "-std=c++17",
+    "-Xcompiler", "-fPIC",
 ]
+FMAD = {"mbm_adjoint.cu": "true"}          # every other source: -fmad=false
 
 
 def nvcc() -> str:
@@ -44,16 +47,33 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     if not force and not _stale():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    procs, objs = [], []
+    for f in SOURCES:                     # one object per source, compiled in parallel
+        obj = os.path.join(objdir, f.replace(".cu", ".o"))
+        cmd = [nvcc(), *NVCC_FLAGS, "-fmad=" + FMAD.get(f, "false")]
+        if ptxas_info:
+            cmd += ["-Xptxas", "-v"]
+        cmd += ["-c", os.path.join(CSRC, f), "-o", obj]
+        procs.append((f, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+        objs.append(obj)
+    failed = []
+    for f, p in procs:
+        out = p.communicate()[0]
+        if verbose or p.returncode != 0:
+            sys.stderr.write(out)
+        if p.returncode != 0:
+            failed.append(f)
+    if failed:
+        raise RuntimeError("nvcc failed on " + ", ".join(failed))
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *NVCC_FLAGS]
-    if ptxas_info:
-        cmd += ["-Xptxas", "-v"]
-    cmd += ["-o", tmp] + [os.path.join(CSRC, f) for f in SOURCES]
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    r = subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *objs],
+                       capture_output=True, text=True)
     if verbose or r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed building libmbm_b200.so")
+        raise RuntimeError("nvcc failed linking libmbm_b200.so")
     os.replace(tmp, LIB)
     return LIB
 

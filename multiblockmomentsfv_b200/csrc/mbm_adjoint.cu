@@ -1,0 +1,287 @@
+// mbm_adjoint.cu -- discrete adjoint of the Heun step (the reverse of Update and
+// SetBoundary), by hand, in three passes per stage over the blocks of a context:
+//
+//   A  projected primitives P of every cell of the stage input (as the forward
+//      stage computes them: Primitive, relaxed with flag 2H+1 off the outermost ring);
+//   B  per face next to an output cell: the flux adjoint
+//         lambda_F = s * dt/h * (lambda_out(right) - lambda_out(left)),  s = 1 or 1/2,
+//      through the HLL flux to the two reconstructed states (PL, PR);
+//   C  per cell: the state adjoints of its faces, through the reconstructions
+//      P +- h/2 S and the limited slopes S = Limit1(d1, d2)/h of itself and its two
+//      neighbours (one-sided derivatives at the limiter's kinks), then through the
+//      relaxation and Primitive to the stage input; the relaxation term R of the
+//      update adds Cons/relax/Primitive adjoints to the input (and to Data0 in
+//      stage 2); the Kn derivative is summed.
+//
+// The ghost fill is linear: its adjoint adds each ghost cell's adjoint, with the
+// wall signs, into the interior cell it was copied from (Dirichlet ghosts have no
+// source and contribute nothing).  dt is frozen from the forward run.
+#include <cuda_runtime.h>
+
+#include "mbm_internal.h"
+#define MBM_HD __host__ __device__ __forceinline__
+#include "mbm_adjoint_math.cuh"
+
+namespace mbm {
+
+__device__ __forceinline__ long long cidx(const BlockDev& B, int I, int J) {
+  return B.off + (long long)J * B.pitch + I + 1;
+}
+
+// which block and cell a flat thread index covers (blocks in order)
+__device__ __forceinline__ bool locate(const BlockDev* blk, int nblk, long long k, int& b, int& I, int& J) {
+  for (b = 0; b < nblk; b++) {
+    const long long n = (long long)blk[b].nxp * blk[b].nyp;
+    if (k < n) {
+      J = (int)(k / blk[b].nxp);
+      I = (int)(k - (long long)J * blk[b].nxp);
+      return true;
+    }
+    k -= n;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void load9(const double* base, const BlockDev& B, int I, int J, double* v) {
+  const long long i = cidx(B, I, J);
+#pragma unroll
+  for (int m = 0; m < NV; m++) v[m] = base[i + m * B.plane];
+}
+
+// pass A: the forward stage's projected primitives (Aux.Prim, src/Main.c:314-336)
+__global__ void adj_prims(AdjArgs a, long long ncell) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b, I, J;
+  if (k >= ncell || !locate(a.blk, a.nblk, k, b, I, J)) return;
+  const BlockDev B = a.blk[b];
+  double U[NV], P[NV];
+  load9(a.x, B, I, J, U);
+  mbm_adj::prim(U, P);
+  const bool ring = I == 0 || J == 0 || I == B.nxp - 1 || J == B.nyp - 1;
+  if (!ring) {
+    double Q[NV];
+    mbm_adj::relax_p(P, Q, a.dt, a.Kn, a.F, 2 * a.heun + 1);
+#pragma unroll
+    for (int m = 0; m < NV; m++) P[m] = Q[m];
+  }
+  const long long i = cidx(B, I, J);
+#pragma unroll
+  for (int m = 0; m < NV; m++) a.P[i + m * B.plane] = P[m];
+}
+
+__device__ __forceinline__ bool inner(const BlockDev& B, int I, int J) {
+  return I >= NG && I <= B.nxp - 1 - NG && J >= NG && J <= B.nyp - 1 - NG;
+}
+
+// limited slope of cell (I,J) along dir from the primitives (src/Main.c:346-349)
+__device__ __forceinline__ double slope_at(const AdjArgs& a, const BlockDev& B, int I, int J, int dir, int m,
+                                          double h) {
+  const long long i = cidx(B, I, J) + m * B.plane;
+  const long long s = dir == 1 ? 1 : B.pitch;
+  const double d1 = a.P[i] - a.P[i - s], d2 = a.P[i + s] - a.P[i];
+  return mbm_adj::limit_val(a.limiter, d1, d2) / h;
+}
+
+// pass B: faces (I,J)|(I+1,J) (dir 1) or (I,J)|(I,J+1) (dir 2) next to an output cell
+__global__ void adj_faces(AdjArgs a, long long ncell, int dir) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b, I, J;
+  if (k >= ncell || !locate(a.blk, a.nblk, k, b, I, J)) return;
+  const BlockDev B = a.blk[b];
+  const int I2 = dir == 1 ? I + 1 : I, J2 = dir == 1 ? J : J + 1;
+  const bool face = I2 < B.nxp && J2 < B.nyp;
+  const bool inL = inner(B, I, J), inR = face && inner(B, I2, J2);
+  if (!inL && !inR) {            // no output cell next to this face: zero adjoint
+    const long long i = cidx(B, I, J);
+#pragma unroll
+    for (int m = 0; m < NV; m++) {
+      a.FL[i + m * B.plane] = 0.0;
+      a.FR[i + m * B.plane] = 0.0;
+    }
+    return;
+  }
+  const double h = dir == 1 ? B.dx : B.dy;
+  const double s = a.heun ? 0.5 : 1.0;
+  double PL[NV], PR[NV], fb[NV], gl[NV] = {0}, gr[NV] = {0};
+  bool any = false;
+  for (int m = 0; m < NV; m++) {
+    const double lo = inL ? a.lout[cidx(B, I, J) + m * B.plane] : 0.0;
+    const double hi = inR ? a.lout[cidx(B, I2, J2) + m * B.plane] : 0.0;
+    fb[m] = s * a.dt / h * (hi - lo);
+    any = any || fb[m] != 0.0;
+    PL[m] = a.P[cidx(B, I, J) + m * B.plane] + 0.5 * h * slope_at(a, B, I, J, dir, m, h);
+    PR[m] = a.P[cidx(B, I2, J2) + m * B.plane] - 0.5 * h * slope_at(a, B, I2, J2, dir, m, h);
+  }
+  if (any) mbm_adj::hll_p_adj(PL, PR, fb, gl, gr, dir);
+  const long long i = cidx(B, I, J);
+#pragma unroll
+  for (int m = 0; m < NV; m++) {
+    a.FL[i + m * B.plane] = gl[m];
+    a.FR[i + m * B.plane] = gr[m];
+  }
+}
+
+// adjoint of the reconstruction and slopes along one direction, accumulated into Pb
+__device__ __forceinline__ void gather_dir(const AdjArgs& a, const BlockDev& B, int I, int J, int dir,
+                                           const double* FL, const double* FR, double* Pb) {
+  const long long s = dir == 1 ? 1 : B.pitch;
+  const int n = dir == 1 ? B.nxp : B.nyp, c = dir == 1 ? I : J;
+  const double h = dir == 1 ? B.dx : B.dy;
+  const long long i0 = cidx(B, I, J);
+  for (int m = 0; m < NV; m++) {
+    const long long i = i0 + m * B.plane;
+    auto fl = [&](int off) { const int q = c + off; return (q >= 0 && q < n) ? FL[i + off * s] : 0.0; };
+    auto fr = [&](int off) { const int q = c + off; return (q >= 0 && q < n) ? FR[i + off * s] : 0.0; };
+    auto lam_s = [&](int off) { return 0.5 * h * (fl(off) - fr(off - 1)); };   // adjoint of S(c+off)
+    // direct: left state of face c|c+1, right state of face c-1|c
+    double g = fl(0) + fr(-1);
+    // through the slopes of c-1, c, c+1 (each on the cells it reads)
+    for (int off = -1; off <= 1; off++) {
+      const int q = c + off;
+      if (q < 1 || q > n - 2) continue;
+      const double lsv = lam_s(off);
+      if (lsv == 0.0) continue;
+      const long long iq = i + off * s;
+      const double d1 = a.P[iq] - a.P[iq - s], d2 = a.P[iq + s] - a.P[iq];
+      double g1, g2;
+      mbm_adj::limit_grad(a.limiter, d1, d2, &g1, &g2);
+      // S(q) = L(P(q)-P(q-1), P(q+1)-P(q)) / h
+      if (off == 0) g += lsv * (g1 - g2) / h;
+      if (off == -1) g += lsv * g2 / h;
+      if (off == 1) g -= lsv * g1 / h;
+    }
+    Pb[m] += g;
+  }
+}
+
+// pass C: per cell, back to the stage input (and Data0)
+__global__ void adj_cells(AdjArgs a, long long ncell, const double* FLx, const double* FRx, const double* FLy,
+                          const double* FRy) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b, I, J;
+  if (k >= ncell || !locate(a.blk, a.nblk, k, b, I, J)) return;
+  const BlockDev B = a.blk[b];
+  double Pb[NV] = {0}, Ub[NV] = {0}, U[NV], P0[NV];
+  double knb = 0.0;
+  const bool ring = I == 0 || J == 0 || I == B.nxp - 1 || J == B.nyp - 1;
+  if (!ring) {
+    gather_dir(a, B, I, J, 1, FLx, FRx, Pb);
+    gather_dir(a, B, I, J, 2, FLy, FRy, Pb);
+  }
+  load9(a.x, B, I, J, U);
+  mbm_adj::prim(U, P0);
+  double Qb[NV] = {0};
+  bool anyP = false;
+#pragma unroll
+  for (int m = 0; m < NV; m++) anyP = anyP || Pb[m] != 0.0;
+  if (anyP) {     // Aux = relax(Primitive(U), 2H+1) off the ring (ring cells never reach a face)
+    mbm_adj::relax_p_adj(P0, Pb, Qb, &knb, a.dt, a.Kn, 2 * a.heun + 1);
+  }
+  if (inner(B, I, J)) {
+    // update term R: Conservative(relax(Primitive(X), 2H)) [+ Conservative(relax(Primitive(D0), -1))]
+    const double s = a.heun ? 0.5 : 1.0;
+    double Rb[NV], Q[NV], Cb[NV] = {0};
+#pragma unroll
+    for (int m = 0; m < NV; m++) Rb[m] = s * a.lout[cidx(B, I, J) + m * B.plane];
+    mbm_adj::relax_p(P0, Q, a.dt, a.Kn, a.F, 2 * a.heun);
+    mbm_adj::cons_adj(Q, Rb, Cb);
+    mbm_adj::relax_p_adj(P0, Cb, Qb, &knb, a.dt, a.Kn, 2 * a.heun);
+    if (a.heun) {
+      double V[NV], W[NV], Q2[NV], C2[NV] = {0}, Pd[NV] = {0}, Vb[NV] = {0};
+      load9(a.d0, B, I, J, V);
+      mbm_adj::prim(V, W);
+      mbm_adj::relax_p(W, Q2, a.dt, a.Kn, a.F, -1);
+      mbm_adj::cons_adj(Q2, Rb, C2);
+      mbm_adj::relax_p_adj(W, C2, Pd, &knb, a.dt, a.Kn, -1);
+      mbm_adj::prim_adj(V, Pd, Vb);
+      const long long i = cidx(B, I, J);
+#pragma unroll
+      for (int m = 0; m < NV; m++) a.ld0[i + m * B.plane] += Vb[m];
+    }
+  }
+  bool anyQ = false;
+#pragma unroll
+  for (int m = 0; m < NV; m++) anyQ = anyQ || Qb[m] != 0.0;
+  if (anyQ) {     // cells no stage output depends on may hold no state (zero density)
+    mbm_adj::prim_adj(U, Qb, Ub);
+    const long long i = cidx(B, I, J);
+#pragma unroll
+    for (int m = 0; m < NV; m++) a.lx[i + m * B.plane] += Ub[m];
+  }
+  // the Kn derivative: warp sum, one atomic per warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) knb += __shfl_xor_sync(0xffffffffu, knb, o);
+  if ((threadIdx.x & 31) == 0 && knb != 0.0) atomicAdd(a.knb, knb);
+}
+
+// adjoint of the ghost fill: ghost adjoint -> its source cell (wall signs), then zero
+__global__ void adj_ghosts(const BlockDev* __restrict__ blk, const GhostEntry* __restrict__ map, int n, double* l) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const GhostEntry e = map[i];
+  const BlockDev D = blk[e.dst_blk];
+  const int sblk = e.src_blk_flags & 0xffff;
+  const bool fx = (e.src_blk_flags >> 16) & 1, fy = (e.src_blk_flags >> 17) & 1;
+  for (int m = 0; m < NV; m++) {
+    double* g = l + D.off + e.dst + m * D.plane;
+    const double v = *g;
+    *g = 0.0;
+    if (e.src < 0 || v == 0.0) continue;       // Dirichlet ghosts have no source
+    const BlockDev S = blk[sblk];
+    const bool flip = (fx && (m == 1 || m == 5 || m == 7)) != (fy && (m == 2 || m == 5 || m == 8));
+    atomicAdd(l + S.off + e.src + m * S.plane, flip ? -v : v);
+  }
+}
+
+// dJ/dU of J = sum over interior cells of q1^2 + q2^2 (heat flux of the final state)
+__global__ void adj_functional(const BlockDev* __restrict__ blk, int nblk, const double* x, double* l,
+                               long long ncell, double* J) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b, I, Jj;
+  double jv = 0.0;
+  if (k < ncell && locate(blk, nblk, k, b, I, Jj)) {
+    const BlockDev B = blk[b];
+    if (inner(B, I, Jj)) {
+      double U[NV], P[NV], Pb[NV] = {0}, Ub[NV] = {0};
+      load9(x, B, I, Jj, U);
+      mbm_adj::prim(U, P);
+      jv = P[7] * P[7] + P[8] * P[8];
+      Pb[7] = 2 * P[7];
+      Pb[8] = 2 * P[8];
+      mbm_adj::prim_adj(U, Pb, Ub);
+      const long long i = cidx(B, I, Jj);
+      for (int m = 0; m < NV; m++) l[i + m * B.plane] = Ub[m];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) jv += __shfl_xor_sync(0xffffffffu, jv, o);
+  if ((threadIdx.x & 31) == 0 && jv != 0.0) atomicAdd(J, jv);
+}
+
+cudaError_t adjoint_stage(const AdjArgs& a0, long long ncell, double* FLx, double* FRx, double* FLy,
+                          double* FRy, cudaStream_t s) {
+  const int T = 128;
+  const unsigned G = (unsigned)((ncell + T - 1) / T);
+  adj_prims<<<G, T, 0, s>>>(a0, ncell);
+  AdjArgs a = a0;
+  a.FL = FLx; a.FR = FRx;
+  adj_faces<<<G, T, 0, s>>>(a, ncell, 1);
+  a.FL = FLy; a.FR = FRy;
+  adj_faces<<<G, T, 0, s>>>(a, ncell, 2);
+  adj_cells<<<G, T, 0, s>>>(a0, ncell, FLx, FRx, FLy, FRy);
+  return cudaGetLastError();
+}
+
+cudaError_t adjoint_ghosts(const BlockDev* blk, const GhostEntry* map, int n, double* l, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  adj_ghosts<<<(n + 127) / 128, 128, 0, s>>>(blk, map, n, l);
+  return cudaGetLastError();
+}
+
+cudaError_t adjoint_functional(const BlockDev* blk, int nblk, const double* x, double* l, long long ncell,
+                               double* J, cudaStream_t s) {
+  adj_functional<<<(unsigned)((ncell + 127) / 128), 128, 0, s>>>(blk, nblk, x, l, ncell, J);
+  return cudaGetLastError();
+}
+
+}  // namespace mbm

@@ -26,9 +26,18 @@ cudaError_t launch_control(CaseDev* cases, int ncases, const BlockDev* blk, unsi
                            double* trace, int* queues, cudaGraphConditionalHandle h, int use_handle,
                            cudaStream_t s);
 int stage_ctas_per_sm();
+cudaError_t launch_ckpt(const CaseDev* cases, const double* buf0, const double* buf1, long long layer_elems,
+                        int grid, cudaStream_t s);
+cudaError_t adjoint_stage(const AdjArgs& a0, long long ncell, double* FLx, double* FRx, double* FLy,
+                          double* FRy, cudaStream_t s);
+cudaError_t adjoint_ghosts(const BlockDev* blk, const GhostEntry* map, int n, double* l, cudaStream_t s);
+cudaError_t adjoint_functional(const BlockDev* blk, int nblk, const double* x, double* l, long long ncell,
+                               double* J, cudaStream_t s);
 cudaError_t launch_fill_uniform(double* base, long long plane, cudaStream_t s);
 cudaError_t launch_stage_cfl(const BlockDev* blk, int nblk, const CaseDev* cases,
                              unsigned long long* lam, int stage, double* out, cudaStream_t s);
+cudaError_t launch_output_fields(const double* src, int nxp, int nyp, int pitch, long long plane, int single,
+                                 void* dst, cudaStream_t s);
 cudaError_t launch_aos_to_planes(const double* aos, double* dst, int nxp, int nyp, int pitch,
                                  long long plane, cudaStream_t s);
 cudaError_t launch_planes_to_aos(const double* src, double* aos, int nxp, int nyp, int pitch,
@@ -81,6 +90,16 @@ struct mbm_ctx {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   bool host_loop = false;           // MBM_HOST_LOOP=1: drive the step loop from the host
+  bool adjoint = false;             // graph body records checkpoints and dt (mbm_params.adjoint)
+  // adjoint work space (allocated on first use)
+  double* adj_buf[8] = {nullptr};   // two adjoint layers, primitives, 4 face-adjoint layers, spare
+  double* adj_ckpt = nullptr;
+  double* adj_seg = nullptr;         // DATA states of one checkpoint segment
+  double* adj_segT = nullptr;        // their stage-1 (TMP) states
+  double* adj_dtlog = nullptr;
+  double* adj_scal = nullptr;       // [0] dJ/dKn, [1] J
+  double* adj_dtrep = nullptr;      // dt values of mbm_replay
+  int adj_nsteps = 0, adj_every = 0, adj_nrep = 0;
   std::string err;
 };
 
@@ -132,7 +151,9 @@ static int validate(const mbm_block_desc* b, int n, std::string& why, int lo = 0
     if (b[i].nx < 1 || b[i].ny < 1 || b[i].nx > (1 << 20) || b[i].ny > (1 << 20)) {
       why = "block " + std::to_string(i + 1) + ": bad cell counts"; return MBM_EINVAL;
     }
-    if (!(b[i].dx > 0) || !(b[i].dy > 0)) { why = "block " + std::to_string(i + 1) + ": dx, dy must be > 0"; return MBM_EINVAL; }
+    if (!(b[i].dx > 1e-100 && b[i].dx < 1e100) || !(b[i].dy > 1e-100 && b[i].dy < 1e100)) {
+      why = "block " + std::to_string(i + 1) + ": dx, dy must be in (1e-100, 1e100)"; return MBM_EINVAL;
+    }
     for (int s = 0; s < 4; s++) {
       int code = b[i].bc[s];
       if (code > 0 && (code - 1 < lo || code - 1 >= hi)) { why = "block " + std::to_string(i + 1) + ": sync partner " + std::to_string(code) + " does not exist"; return MBM_EINVAL; }
@@ -295,14 +316,15 @@ static int set_segments(mbm_ctx* c, int seg) {
 }
 
 // one Heun stage of every block: one persistent launch per limiter group
-static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, int sel_out) {
+static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, int sel_out,
+                                 double* const* bufs = nullptr) {
   for (const LimGroup& g : c->groups) {
     StageArgs a{};
     a.blk = c->dblk;
     a.work = c->dwork + g.start;
     a.nwork = g.count;
     a.cases = c->dcase;
-    for (int l = 0; l < 3; l++) a.buf[l] = c->buf[l];
+    for (int l = 0; l < 3; l++) a.buf[l] = bufs ? bufs[l] : c->buf[l];
     a.lam = c->dlam;
     a.queue = c->dqueue + heun * 5 + g.lim;
     a.sel_in = sel_in; a.sel_d0 = sel_d0; a.sel_out = sel_out;
@@ -320,11 +342,17 @@ static cudaError_t launch_attempt(mbm_ctx* c, cudaGraphConditionalHandle h, int 
   if ((e = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_TMP, c->stream))) return e;
   if ((e = launch_stages(c, 1, SEL_TMP, SEL_CUR, SEL_OTHER))) return e;
   if ((e = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_OTHER, c->stream))) return e;
-  return launch_control(c->dcase, c->ncase, c->dblk, c->dlam, c->dtrace, c->dqueue, h, use_handle, c->stream);
+  if ((e = launch_control(c->dcase, c->ncase, c->dblk, c->dlam, c->dtrace, c->dqueue, h, use_handle, c->stream)))
+    return e;
+  if (c->adjoint) return launch_ckpt(c->dcase, c->buf[0], c->buf[1], c->layer_elems, 4 * c->nsm, c->stream);
+  return cudaSuccess;
 }
 
 static int push_cases(mbm_ctx* c) {
   CK(cudaMemcpyAsync(c->dcase, c->hcase, sizeof(CaseDev) * c->ncase, cudaMemcpyHostToDevice, c->stream));
+  // the records are pinned: the copy reads them when the stream reaches it, so the
+  // host must not change them before then
+  CK(cudaStreamSynchronize(c->stream));
   return MBM_OK;
 }
 
@@ -366,7 +394,7 @@ static int autotune(mbm_ctx* c) {
     if (it != g_tune_cache.end()) return set_segments(c, it->second);
   }
   const char* env = getenv("MBM_AUTOTUNE");
-  if ((env && atoi(env) == 0) || cells < 200000) return set_segments(c, 32);
+  if (env && atoi(env) == 0) return set_segments(c, 32);
   for (int l = 0; l < 3; l++)
     for (auto& d : c->hblk) CK(launch_fill_uniform(c->buf[l] + d.off, d.plane, c->stream));
   for (int k = 0; k < c->ncase; k++) {
@@ -380,7 +408,8 @@ static int autotune(mbm_ctx* c) {
   CK(cudaEventCreate(&e1));
   int best = 32;
   float best_ms = 1e30f;
-  for (int seg : {16, 24, 32, 48, 64, 96}) {
+  // short segments buy parallelism on small grids, long ones save warm-up rows
+  for (int seg : {8, 12, 16, 24, 32, 48, 64}) {
     st = set_segments(c, seg);
     float ms = 0.f;
     if (!st) st = time_both_stages(c, e0, e1, &ms);
@@ -416,7 +445,7 @@ extern "C" int mbm_create_batch(const mbm_block_desc* blocks, int nblocks, const
     if (cd.nblocks < 1 || cd.first_block < 0 || cd.first_block + cd.nblocks > nblocks)
       return fail(nullptr, MBM_EINVAL, "case " + std::to_string(k) + ": block range outside the table");
     if (cd.limiter < 0 || cd.limiter > 4) return fail(nullptr, MBM_EINVAL, "limiter code must be 0..4");
-    if (!(cd.Kn > 0)) return fail(nullptr, MBM_EINVAL, "Kn must be > 0");
+    if (!(cd.Kn > 1e-100 && cd.Kn < 1e100)) return fail(nullptr, MBM_EINVAL, "Kn must be in (1e-100, 1e100)");
     for (int b = cd.first_block; b < cd.first_block + cd.nblocks; b++) {
       if (blk_case[b] >= 0) return fail(nullptr, MBM_EINVAL, "cases overlap");
       blk_case[b] = k;
@@ -448,6 +477,7 @@ extern "C" int mbm_create_batch(const mbm_block_desc* blocks, int nblocks, const
     c->host_loop = hl && atoi(hl) != 0;
   }
   if (c->prm.max_attempts <= 0) c->prm.max_attempts = 10000000;
+  c->adjoint = params->adjoint != 0 && ncases == 1;
   c->device = params->device;
   c->nblk = nblocks;
   c->ncase = ncases;
@@ -494,7 +524,7 @@ extern "C" int mbm_create_batch(const mbm_block_desc* blocks, int nblocks, const
     CKC(cudaMalloc(&c->buf[l], sizeof(double) * off));
     CKC(cudaMemsetAsync(c->buf[l], 0, sizeof(double) * off, c->stream));
   }
-  CKC(cudaMalloc(&c->staging, sizeof(double) * max_cells * NV));
+  CKC(cudaMalloc(&c->staging, sizeof(double) * max_cells * (NV + 1)));   // layers, or 10 output fields
   CKC(cudaMalloc(&c->dblk, sizeof(BlockDev) * nblocks));
   CKC(cudaMemcpyAsync(c->dblk, c->hblk.data(), sizeof(BlockDev) * nblocks, cudaMemcpyHostToDevice, c->stream));
 
@@ -612,6 +642,13 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   if (c->hcase) cudaFreeHost(c->hcase);
   cudaFree(c->dlam);
   cudaFree(c->dqueue);
+  for (int k = 0; k < 8; k++) cudaFree(c->adj_buf[k]);
+  cudaFree(c->adj_ckpt);
+  cudaFree(c->adj_seg);
+  cudaFree(c->adj_segT);
+  cudaFree(c->adj_dtlog);
+  cudaFree(c->adj_dtrep);
+  cudaFree(c->adj_scal);
   cudaFree(c->dtrace);
   cudaFree(c->dcfl);
   if (c->hcfl) cudaFreeHost(c->hcfl);
@@ -647,6 +684,17 @@ extern "C" int mbm_download(mbm_ctx* c, int layer, int block, double* cells) {
   const BlockDev& d = c->hblk[block];
   CK(launch_planes_to_aos(c->buf[phys_of(c, layer, block)] + d.off, c->staging, d.nxp, d.nyp, d.pitch, d.plane, c->stream));
   CK(cudaMemcpyAsync(cells, c->staging, sizeof(double) * d.nxp * d.nyp * NV, cudaMemcpyDeviceToHost, c->stream));
+  return wait_stream(c);
+}
+
+extern "C" int mbm_output_fields(mbm_ctx* c, int block, int single, void* out) {
+  if (!c || !out || block < 0 || block >= c->nblk) return fail(c, MBM_EINVAL, "mbm_output_fields: bad argument");
+  CK(cudaSetDevice(c->device));
+  const BlockDev& d = c->hblk[block];
+  const size_t bytes = (size_t)(d.nxp - 4) * (d.nyp - 4) * 10 * (single ? sizeof(float) : sizeof(double));
+  CK(launch_output_fields(c->buf[phys_of(c, MBM_L_DATA, block)] + d.off, d.nxp, d.nyp, d.pitch, d.plane,
+                          single, c->staging, c->stream));
+  CK(cudaMemcpyAsync(out, c->staging, bytes, cudaMemcpyDeviceToHost, c->stream));
   return wait_stream(c);
 }
 
@@ -737,6 +785,7 @@ extern "C" int mbm_steps_batch(mbm_ctx* c, double* t, const double* tend, double
     h.nstep = h.nrej = h.attempts = 0;
     h.step_cap = max_steps;
     h.status = 0;
+    h.nonfinite = 0;
     h.trace_n = 0;
     h.show_every = c->prm.show_every;
     h.max_attempts = c->prm.max_attempts;
@@ -772,7 +821,7 @@ extern "C" int mbm_steps_batch(mbm_ctx* c, double* t, const double* tend, double
     if (nrej) nrej[k] = h.nrej;
     if (h.status) worst = h.status;
   }
-  if (worst == 2) return fail(c, MBM_ENONFINITE, "CFL or dt became non-finite");
+  if (worst == 2) return fail(c, MBM_ENONFINITE, "a stage wrote NaN or infinity, or CFL or dt became non-finite");
   if (worst == 5) return fail(c, MBM_ESTEPLIMIT, "step attempts exceeded max_attempts");
   return MBM_OK;
 }
@@ -809,6 +858,15 @@ extern "C" int mbm_attempts(mbm_ctx* c, int* attempts) {
   int a = 0;
   for (int k = 0; k < c->ncase; k++) a = std::max(a, c->hcase[k].attempts);
   *attempts = a;
+  return MBM_OK;
+}
+
+extern "C" int mbm_case_status(mbm_ctx* c, int* status, int n) {
+  if (!c || !status || n < 0 || n > c->ncase) return fail(c, MBM_EINVAL, "mbm_case_status: bad argument");
+  for (int k = 0; k < n; k++) {
+    const int s = c->hcase[k].status;
+    status[k] = s == 2 ? MBM_ENONFINITE : s == 5 ? MBM_ESTEPLIMIT : MBM_OK;
+  }
   return MBM_OK;
 }
 
@@ -860,6 +918,240 @@ extern "C" int mbm_trace_case(mbm_ctx* c, int k, double* rec, int cap, int* n) {
   return MBM_OK;
 }
 
+// ------------------------------------------------------------------ adjoint --
+// Discrete adjoint of a Steps run (hand-written reverse of Update and SetBoundary,
+// mbm_adjoint.cu), dt frozen from the forward run, checkpoints every k steps.
+
+static int adj_alloc(mbm_ctx* c, int nsteps, int every) {
+  if (!c->adj_buf[0])
+    for (int k = 0; k < 8; k++) CK(cudaMalloc(&c->adj_buf[k], sizeof(double) * c->layer_elems));
+  if (!c->adj_scal) CK(cudaMalloc(&c->adj_scal, sizeof(double) * 2));
+  if (nsteps > c->adj_nsteps || every != c->adj_every) {
+    cudaFree(c->adj_ckpt);
+    cudaFree(c->adj_seg);
+  cudaFree(c->adj_segT);
+    cudaFree(c->adj_dtlog);
+    c->adj_ckpt = c->adj_seg = c->adj_segT = c->adj_dtlog = nullptr;
+    const int nck = nsteps / every + 1;
+    CK(cudaMalloc(&c->adj_ckpt, sizeof(double) * c->layer_elems * nck));
+    CK(cudaMalloc(&c->adj_seg, sizeof(double) * c->layer_elems * (every + 1)));
+    CK(cudaMalloc(&c->adj_segT, sizeof(double) * c->layer_elems * every));
+    CK(cudaMalloc(&c->adj_dtlog, sizeof(double) * nsteps));
+    c->adj_nsteps = nsteps;
+    c->adj_every = every;
+  }
+  return MBM_OK;
+}
+
+// the case record for frozen-dt stages: buffer selectors relative to cur = 0, not done
+static int frozen_begin(mbm_ctx* c) {
+  CaseDev& h = c->hcase[0];
+  h.cur = 0;
+  h.done = 0;
+  return push_cases(c);
+}
+
+// one frozen-dt Heun step: in (full layer) -> out (full layer) through tmp (the
+// stage-1 state, ghosts filled); out = nullptr stops after stage 1.  ddt points at
+// the step's dt in device memory (copied into the case record on the stream, so
+// consecutive steps queue without a host round trip)
+static int frozen_step(mbm_ctx* c, const double* in, double* out, const double* ddt, double* tmp) {
+  double* bufs[3] = {const_cast<double*>(in), out, tmp};
+  CK(cudaMemcpyAsync(&c->dcase[0].dt, ddt, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
+  CK(launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP, bufs));
+  CK(launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, bufs, c->ddir, SEL_TMP, c->stream));
+  if (!out) return MBM_OK;
+  CK(launch_stages(c, 1, SEL_TMP, SEL_CUR, SEL_OTHER, bufs));
+  CK(launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, bufs, c->ddir, SEL_OTHER, c->stream));
+  return MBM_OK;
+}
+
+static long long ncells(mbm_ctx* c) {
+  long long n = 0;
+  for (auto& d : c->hblk) n += (long long)d.nxp * d.nyp;
+  return n;
+}
+
+// reverse of one step: lam (adjoint of D_{n+1}, interior) -> lam_next (adjoint of
+// D_n); Tn = stage 1 of D_n with its ghost fill
+static int adj_step(mbm_ctx* c, const double* Dn, const double* Tn, double dt, double* lam, double* lam_next) {
+  const size_t bytes = sizeof(double) * c->layer_elems;
+  double* lamT = c->adj_buf[2];
+  double* P = c->adj_buf[3];
+  const long long nc = ncells(c);
+  const CaseDev& h = c->hcase[0];
+  CK(cudaMemsetAsync(lamT, 0, bytes, c->stream));
+  CK(cudaMemsetAsync(lam_next, 0, bytes, c->stream));
+  AdjArgs a{};
+  a.blk = c->dblk;
+  a.nblk = c->nblk;
+  a.P = P;
+  a.knb = c->adj_scal;
+  a.dt = dt;
+  a.Kn = h.Kn;
+  a.F = h.F;
+  a.limiter = h.limiter;
+  // stage 2: NEW = stage2(TMP, D_n)
+  a.heun = 1;
+  a.x = Tn;
+  a.d0 = Dn;
+  a.lout = lam;
+  a.lx = lamT;
+  a.ld0 = lam_next;
+  CK(adjoint_stage(a, nc, c->adj_buf[4], c->adj_buf[5], c->adj_buf[6], c->adj_buf[7], c->stream));
+  CK(adjoint_ghosts(c->dblk, c->dghost, c->nghost, lamT, c->stream));
+  // stage 1: TMP = stage1(D_n)
+  a.heun = 0;
+  a.x = Dn;
+  a.d0 = Dn;
+  a.lout = lamT;
+  a.lx = lam_next;
+  a.ld0 = nullptr;
+  CK(adjoint_stage(a, nc, c->adj_buf[4], c->adj_buf[5], c->adj_buf[6], c->adj_buf[7], c->stream));
+  CK(adjoint_ghosts(c->dblk, c->dghost, c->nghost, lam_next, c->stream));
+  return MBM_OK;
+}
+
+extern "C" int mbm_adjoint_run(mbm_ctx* c, double* t, int nsteps, int every, double CFLreg, double* J,
+                               double* grad, double* grad_Kn, double* dts_out, double* ms) {
+  if (!c || !t || nsteps < 1 || every < 1 || c->ncase != 1) return fail(c, MBM_EINVAL, "mbm_adjoint_run: bad argument");
+  if (!c->adjoint) return fail(c, MBM_EINVAL, "mbm_adjoint_run: context created without mbm_params.adjoint");
+  CK(cudaSetDevice(c->device));
+  int st = adj_alloc(c, nsteps, every);
+  if (st) return st;
+  const size_t bytes = sizeof(double) * c->layer_elems;
+  cudaEvent_t e0, e1, e2;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventCreate(&e2));
+  // forward: Steps with a step cap, recording dt and checkpoints (step 0 = the input state)
+  CaseDev& h = c->hcase[0];
+  CK(cudaMemcpyAsync(c->adj_ckpt, c->buf[h.cur], bytes, cudaMemcpyDeviceToDevice, c->stream));
+  h.ckpt = c->adj_ckpt;
+  h.ckpt_every = every;
+  h.dtlog = c->adj_dtlog;
+  h.dtlog_cap = nsteps;
+  CK(cudaEventRecord(e0, c->stream));
+  int n = 0, r = 0;
+  st = mbm_steps_capped(c, t, 1e300, 1.0, CFLreg, nsteps, &n, &r);
+  h.ckpt = nullptr;
+  h.dtlog = nullptr;
+  h.ckpt_every = 0;
+  h.dtlog_cap = 0;
+  if (st) return st;
+  if ((st = push_cases(c))) return st;
+  CK(cudaEventRecord(e1, c->stream));
+  std::vector<double> dts(n);
+  CK(cudaMemcpy(dts.data(), c->adj_dtlog, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (dts_out) {
+    for (int k = 0; k < nsteps; k++) dts_out[k] = k < n ? dts[k] : 0.0;
+  }
+  // functional and its gradient at the final state
+  double* lam = c->adj_buf[0];
+  double* lam2 = c->adj_buf[1];
+  CK(cudaMemsetAsync(c->adj_scal, 0, sizeof(double) * 2, c->stream));
+  CK(cudaMemsetAsync(lam, 0, bytes, c->stream));
+  CK(adjoint_functional(c->dblk, c->nblk, c->buf[h.cur], lam, ncells(c), c->adj_scal + 1, c->stream));
+  // reverse sweep over segments [s*every, min((s+1)*every, n))
+  const int cur0 = h.cur;
+  if ((st = frozen_begin(c))) return st;
+  for (int s = (n - 1) / every; s >= 0; s--) {
+    const int a = s * every, b = std::min(n, a + every);
+    CK(cudaMemcpyAsync(c->adj_seg, c->adj_ckpt + (size_t)s * c->layer_elems, bytes, cudaMemcpyDeviceToDevice,
+                       c->stream));
+    // recompute the segment's states and stage-1 states (the last step's stage 1 only)
+    for (int k = a; k < b; k++)
+      if ((st = frozen_step(c, c->adj_seg + (size_t)(k - a) * c->layer_elems,
+                            k < b - 1 ? c->adj_seg + (size_t)(k - a + 1) * c->layer_elems : nullptr,
+                            c->adj_dtlog + k, c->adj_segT + (size_t)(k - a) * c->layer_elems)))
+        return st;
+    for (int k = b - 1; k >= a; k--) {
+      if ((st = adj_step(c, c->adj_seg + (size_t)(k - a) * c->layer_elems,
+                         c->adj_segT + (size_t)(k - a) * c->layer_elems, dts[k], lam, lam2)))
+        return st;
+      std::swap(lam, lam2);
+    }
+  }
+  h.cur = cur0;
+  h.done = 1;
+  if ((st = push_cases(c))) return st;
+  // the frozen stages left CFL maxima no controller read: clear them for the next run
+  CK(cudaMemsetAsync(c->dlam, 0, sizeof(unsigned long long) * 6 * c->nblk, c->stream));
+  CK(cudaEventRecord(e2, c->stream));
+  double sc[2];
+  CK(cudaMemcpyAsync(sc, c->adj_scal, sizeof sc, cudaMemcpyDeviceToHost, c->stream));
+  if ((st = wait_stream(c))) return st;
+  float f_ms = 0.f, a_ms = 0.f;
+  CK(cudaEventElapsedTime(&f_ms, e0, e1));
+  CK(cudaEventElapsedTime(&a_ms, e1, e2));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  if (J) *J = sc[1];
+  if (grad_Kn) *grad_Kn = sc[0];
+  if (ms) { ms[0] = f_ms; ms[1] = a_ms; }
+  if (grad) {   // adjoint of the input state, array of structs per block, ghosts zero
+    size_t o = 0;
+    for (int b = 0; b < c->nblk; b++) {
+      const BlockDev& d = c->hblk[b];
+      CK(launch_planes_to_aos(lam + d.off, c->staging, d.nxp, d.nyp, d.pitch, d.plane, c->stream));
+      CK(cudaMemcpyAsync(grad + o, c->staging, sizeof(double) * d.nxp * d.nyp * NV, cudaMemcpyDeviceToHost,
+                         c->stream));
+      if ((st = wait_stream(c))) return st;
+      o += (size_t)d.nxp * d.nyp * NV;
+    }
+  }
+  return MBM_OK;
+}
+
+// frozen-dt forward: n Heun steps of DATA with the given dt values, no controller;
+// *J (may be NULL) receives the heat-flux functional of the result
+extern "C" int mbm_replay(mbm_ctx* c, const double* dts, int n, double* J) {
+  if (!c || (n > 0 && !dts) || n < 0 || c->ncase != 1) return fail(c, MBM_EINVAL, "mbm_replay: bad argument");
+  CK(cudaSetDevice(c->device));
+  CaseDev& h = c->hcase[0];
+  int cur = h.cur, st;
+  if (n > c->adj_nrep) {
+    cudaFree(c->adj_dtrep);
+    c->adj_dtrep = nullptr;
+    c->adj_nrep = 0;
+    CK(cudaMalloc(&c->adj_dtrep, sizeof(double) * n));
+    c->adj_nrep = n;
+  }
+  if (n > 0) CK(cudaMemcpyAsync(c->adj_dtrep, dts, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  if ((st = frozen_begin(c))) return st;     // also orders the dt copy before the host returns
+  for (int k = 0; k < n; k++) {
+    if ((st = frozen_step(c, c->buf[cur], c->buf[1 - cur], c->adj_dtrep + k, c->buf[2]))) return st;
+    cur = 1 - cur;
+  }
+  h.cur = cur;
+  h.done = 1;
+  if ((st = push_cases(c))) return st;
+  CK(cudaMemsetAsync(c->dlam, 0, sizeof(unsigned long long) * 6 * c->nblk, c->stream));
+  if (J) {
+    if (!c->adj_buf[0]) CK(cudaMalloc(&c->adj_buf[0], sizeof(double) * c->layer_elems));
+    if (!c->adj_scal) CK(cudaMalloc(&c->adj_scal, sizeof(double) * 2));
+    CK(cudaMemsetAsync(c->adj_scal, 0, sizeof(double) * 2, c->stream));
+    CK(adjoint_functional(c->dblk, c->nblk, c->buf[cur], c->adj_buf[0], ncells(c), c->adj_scal + 1, c->stream));
+    double sc[2];
+    CK(cudaMemcpyAsync(sc, c->adj_scal, sizeof sc, cudaMemcpyDeviceToHost, c->stream));
+    if ((st = wait_stream(c))) return st;
+    *J = sc[1];
+  }
+  return wait_stream(c);
+}
+
+// Kn and F of every case (the globals the reference's Steps reads)
+extern "C" int mbm_set_physics(mbm_ctx* c, double Kn, double F) {
+  if (!c || !(Kn > 1e-100 && Kn < 1e100)) return fail(c, MBM_EINVAL, "mbm_set_physics: bad argument");
+  for (int k = 0; k < c->ncase; k++) {
+    c->hcase[k].Kn = Kn;
+    c->hcase[k].F = F;
+  }
+  return push_cases(c);
+}
+
 // ------------------------------------------------------------------- misc --
 extern "C" int mbm_ghost_map(const mbm_block_desc* blocks, int nblocks, int* entries, int cap, int* n) {
   std::string why;
@@ -885,7 +1177,7 @@ extern "C" const char* mbm_strerror(int s) {
   switch (s) {
     case MBM_OK: return "ok";
     case MBM_EINVAL: return "invalid argument";
-    case MBM_ENONFINITE: return "non-finite CFL or time step";
+    case MBM_ENONFINITE: return "non-finite state, CFL or time step";
     case MBM_ETIMEOUT: return "device wait timed out";
     case MBM_ECUDA: return "CUDA error";
     case MBM_ENOMEM: return "device out of memory";

@@ -51,7 +51,11 @@ struct CaseDev {       // per-case step controller (src/Main.c:189-244)
   int done, status;
   int show_every, trace_n;
   int blk0, nblk;      // the case's blocks are blk0 .. blk0+nblk-1
-  int pad_;
+  int nonfinite;       // set by a stage that wrote a NaN or infinity
+  int ckpt_every;      // > 0: copy DATA to ckpt[nstep / ckpt_every] every that many steps
+  int dtlog_cap;       // accepted dt values recorded into dtlog (adjoint runs)
+  double* dtlog;
+  double* ckpt;        // checkpoint layers (layer_elems doubles each)
 };
 
 struct StageArgs {
@@ -64,6 +68,22 @@ struct StageArgs {
   int* queue;                // work-item counter of this stage (zero before the launch)
   int sel_in, sel_d0, sel_out;
   int heun;
+};
+
+struct AdjArgs {       // one stage of the discrete adjoint (mbm_adjoint.cu)
+  const BlockDev* blk;
+  int nblk;
+  const double* x;       // stage input layer (all cells)
+  const double* d0;      // Data0 (stage 2)
+  const double* lout;    // adjoint of the stage output (interior cells)
+  double* lx;            // += adjoint of the stage input (all cells)
+  double* ld0;           // += adjoint of Data0 (stage 2)
+  double* P;             // projected primitives of the stage input (layer layout)
+  double* FL;            // adjoint of the left/lower state of each face, at its left/lower cell
+  double* FR;            // adjoint of the right/upper state
+  double* knb;           // += dJ/dKn
+  double dt, Kn, F;
+  int limiter, heun;
 };
 
 __host__ __device__ inline int phys_layer(int sel, int cur) {

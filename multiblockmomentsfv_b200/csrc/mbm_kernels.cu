@@ -69,9 +69,10 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   const bool col_out = lane >= 2 && lane <= 29 && C >= NG && C <= nxp - 1 - NG;
   const bool ylane = lane >= 2 && lane <= 29;        // owners of this strip's y faces
   const double dtdx = dt / B.dx, dtdy = dt / B.dy;
-  const Recip rdx(B.dx), rdy(B.dy);
+  const Recip rdx(B.dx), rdy(B.dy);   // dx, dy in the safe range (checked at creation)
   const double hdx = 0.5 * B.dx, hdy = 0.5 * B.dy;
   double lamx = 0.0, lamy = 0.0, prod = 0.0;
+  bool nonfinite = false;
 
   // The march: iteration r forms the primitives of row r, the y slope of row r-1
   // and the y face (r-2 | r-1), then finishes row J = r-2 (x face, update).
@@ -102,13 +103,27 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     double G[NV];
     const bool face_now = r >= rs + 3;
     if (r >= rs + 2) {
-      double hi[NV];
+      double hi[NV], S[NV];
+      bool sbad = false;
 #pragma unroll
       for (int n = 0; n < NV; n++) {
         const double pm = win.P[sm2][n][lane], p0 = win.P[sm1][n][lane], pp = win.P[s0][n][lane];
-        const double S = rdy.div(limit<LIM>(p0 - pm, pp - p0));
-        hi[n] = p0 - hdy * S;
-        G[n] = p0 + hdy * S;                  // lower state of the next face, parked in G
+        const double L = limit<LIM>(p0 - pm, pp - p0);
+        sbad |= !mk_in(L);
+        S[n] = mk_div(L, rdy.y, rdy.r);
+      }
+      if (__builtin_expect(sbad, 0)) {
+#pragma unroll
+        for (int n = 0; n < NV; n++) {
+          const double pm = win.P[sm2][n][lane], p0 = win.P[sm1][n][lane], pp = win.P[s0][n][lane];
+          S[n] = div_ieee(limit<LIM>(p0 - pm, pp - p0), rdy.y);
+        }
+      }
+#pragma unroll
+      for (int n = 0; n < NV; n++) {
+        const double p0 = win.P[sm1][n][lane];
+        hi[n] = p0 - hdy * S[n];
+        G[n] = p0 + hdy * S[n];               // lower state of the next face, parked in G
       }
       if (face_now && ylane) {
         double lo[NV];
@@ -129,12 +144,26 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     const int J = r - 2;
     if (J >= w.J0 && J < w.J1) {
       double P0[NV], Sx[NV], lo[NV], hi[NV], F[NV];
+      bool xbad = false;
 #pragma unroll
       for (int n = 0; n < NV; n++) {
         P0[n] = win.P[sm2][n][lane];
         const double pl = __shfl_up_sync(0xffffffffu, P0[n], 1);
         const double pr = __shfl_down_sync(0xffffffffu, P0[n], 1);
-        Sx[n] = rdx.div(limit<LIM>(P0[n] - pl, pr - P0[n]));
+        const double L = limit<LIM>(P0[n] - pl, pr - P0[n]);
+        xbad |= !mk_in(L);
+        Sx[n] = mk_div(L, rdx.y, rdx.r);
+      }
+      if (__builtin_expect(__any_sync(0xffffffffu, xbad), 0)) {   // warp-uniform cold path
+#pragma unroll
+        for (int n = 0; n < NV; n++) {
+          const double pl = __shfl_up_sync(0xffffffffu, P0[n], 1);
+          const double pr = __shfl_down_sync(0xffffffffu, P0[n], 1);
+          Sx[n] = div_ieee(limit<LIM>(P0[n] - pl, pr - P0[n]), rdx.y);
+        }
+      }
+#pragma unroll
+      for (int n = 0; n < NV; n++) {
         lo[n] = P0[n] + hdx * Sx[n];
         hi[n] = __shfl_down_sync(0xffffffffu, P0[n] - hdx * Sx[n], 1);
       }
@@ -171,6 +200,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
           v -= dtdx * F[n];
           if (HEUN == 1) v = 0.5 * v;
           out[n * plane + idx] = v;
+          nonfinite |= (__double2hiint(v) & 0x7ff00000) == 0x7ff00000;
         }
       }
     }
@@ -189,6 +219,8 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     lamy = fmax(lamy, __shfl_xor_sync(0xffffffffu, lamy, o));
     prod = fmax(prod, __shfl_xor_sync(0xffffffffu, prod, o));
   }
+  // failure detection: a NaN or infinity in a written cell marks the case
+  if (__any_sync(0xffffffffu, nonfinite) && lane == 0) atomicOr(&a.cases[B.case_id].nonfinite, 1);
   if (lane == 0) {
     unsigned long long* slot = a.lam + ((size_t)w.blk * 2 + HEUN) * 3;
     if (lamx > 0.0) atomicMax(slot + 0, (unsigned long long)__double_as_longlong(lamx));
@@ -280,7 +312,10 @@ __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __res
     const double cfl = rmax(cfl1, rmax(cfl2, 0.0));
     cs.cfl_last = cfl;
     cs.attempts++;
-    if (cfl > cs.CFLmax) {
+    if (cs.nonfinite) {       // a stage wrote a NaN or infinity: stop before accepting it
+      cs.status = 2;          // MBM_ENONFINITE
+      cs.done = 1;
+    } else if (cfl > cs.CFLmax) {
       cs.dt = dt * cs.CFLreg / cfl;
       cs.nrej++;
     } else {
@@ -290,6 +325,7 @@ __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __res
       cs.dt = nd;
       cs.nstep++;
       cs.cur = 1 - cs.cur;
+      if (cs.dtlog && cs.nstep <= cs.dtlog_cap) cs.dtlog[cs.nstep - 1] = dt;   // frozen for the adjoint
       if (cs.show_every > 0 && cs.nstep % cs.show_every == 0 && cs.trace_n < MAX_TRACE) {
         double* r = trace + ((size_t)c * MAX_TRACE + cs.trace_n) * 4;
         r[0] = cs.nstep; r[1] = cfl; r[2] = cs.t; r[3] = cs.dt;
@@ -310,6 +346,25 @@ __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __res
   }
   live = __syncthreads_or(live);
   if (use_handle && threadIdx.x == 0) cudaGraphSetConditional(h, live ? 1u : 0u);
+}
+
+// checkpoint of DATA after every ckpt_every-th accepted step (adjoint runs); a
+// rejected attempt copies the same DATA again
+__global__ void ckpt_kernel(const CaseDev* __restrict__ cases, const double* buf0, const double* buf1,
+                            long long layer_elems) {
+  const CaseDev& cs = cases[0];
+  if (!cs.ckpt || cs.ckpt_every <= 0 || cs.nstep == 0 || cs.nstep % cs.ckpt_every) return;
+  const double* src = cs.cur ? buf1 : buf0;
+  double* dst = cs.ckpt + (size_t)(cs.nstep / cs.ckpt_every) * layer_elems;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < layer_elems;
+       k += (long long)gridDim.x * blockDim.x)
+    dst[k] = src[k];
+}
+
+cudaError_t launch_ckpt(const CaseDev* cases, const double* buf0, const double* buf1, long long layer_elems,
+                        int grid, cudaStream_t s) {
+  ckpt_kernel<<<grid, 256, 0, s>>>(cases, buf0, buf1, layer_elems);
+  return cudaGetLastError();
 }
 
 // CFL of one stage per block, for the single-stage entry points
@@ -335,6 +390,42 @@ __global__ void fill_block_uniform(double* __restrict__ base, long long plane) {
 
 cudaError_t launch_fill_uniform(double* base, long long plane, cudaStream_t s) {
   fill_block_uniform<<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(base, plane);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- output fields --
+// Output's payload on the device (src/Output.c:195-243): for the interior plus one
+// ghost ring, x outer / y inner, the fields rho vx vy T p Pxx Pxy Pyy qx qy of
+// Primitive(U), variables fastest, as float (rounded like the reference's cast) or
+// double.
+__global__ void output_fields(const double* __restrict__ src, int nxp, int nyp, int pitch, long long plane,
+                              int single, void* __restrict__ dst) {
+  const int ni = nyp - 4, nj = nxp - 4;          // points per column (y), columns (x)
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= (long long)ni * nj) return;
+  const int i = (int)(p / ni), j = (int)(p - (long long)i * ni);   // x index outer, y inner
+  const int I = 2 + i, J = 2 + j;
+  double U[NV], P[NV];
+#pragma unroll
+  for (int m = 0; m < NV; m++) U[m] = src[m * plane + (long long)J * pitch + I + 1];
+  primitive(U, P);
+  const double v[10] = {P[0], P[1], P[2], P[3], P[0] * P[3], P[0] * P[4],
+                        P[0] * P[5], P[0] * P[6], P[7], P[8]};
+  if (single) {
+    float* o = (float*)dst + p * 10;
+#pragma unroll
+    for (int m = 0; m < 10; m++) o[m] = (float)v[m];
+  } else {
+    double* o = (double*)dst + p * 10;
+#pragma unroll
+    for (int m = 0; m < 10; m++) o[m] = v[m];
+  }
+}
+
+cudaError_t launch_output_fields(const double* src, int nxp, int nyp, int pitch, long long plane, int single,
+                                 void* dst, cudaStream_t s) {
+  const long long n = (long long)(nyp - 4) * (nxp - 4);
+  output_fields<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(src, nxp, nyp, pitch, plane, single, dst);
   return cudaGetLastError();
 }
 

@@ -28,45 +28,72 @@ __device__ __forceinline__ double rsgn(double a) { return a == 0 ? 0.0 : (a < 0 
 // with r = RN(1/y) and q = RN(x*r), the remainder e = x - q*y is exact in one FMA
 // and RN(q + e*r) = RN(x/y), provided x, y and the quotient stay in the normal
 // range.  One reciprocal then serves every quotient with the same denominator at
-// three FP64 operations each, instead of a full division per quotient, with the
-// same bits as IEEE x/y.  The guards keep |exponent| < 480 for x and y (integer
-// pipe only); zero numerators return x*r (the signed zero of x/y); anything else
-// falls back to IEEE division.  Checked against x/y on the host for 2e8 random
-// operand pairs and by every bitwise parity test.
-__device__ __forceinline__ bool div_range_ok(double y) {
-  const unsigned e = (unsigned)(__double_as_longlong(y) >> 52) & 0x7ffu;
-  return e - 543u <= 960u;
+// three FP64 operations each, with the same bits as IEEE x/y.  The quotient is
+// formed without a branch; a range flag (integer pipe only: |exponent| < 480 for
+// x and y, or x = 0) is collected per function, and a function whose flag is set
+// recomputes its quotients with IEEE division in a cold, outlined path.  Zero
+// numerators take x*r, the signed zero of x/y.  Checked against x/y on the host
+// for 2e8 random operand pairs and by every bitwise parity test.
+__device__ __forceinline__ bool mk_in(double x) {
+  const long long b = __double_as_longlong(x);
+  return (((unsigned)(b >> 52) & 0x7ffu) - 543u <= 960u) || ((b << 1) == 0);
 }
+
+__device__ __forceinline__ double mk_div(double x, double y, double r) {
+  const double q = x * r;
+  const double m = fma(fma(-q, y, x), r, q);
+  return ((__double_as_longlong(x) << 1) == 0) ? q : m;
+}
+
+__device__ __noinline__ double div_ieee(double x, double y) { return x / y; }
 
 struct Recip {        // 1/y for a denominator shared by several quotients
   double y, r;
-  bool ok;
+  bool bad;           // set when any quotient left the safe range
   __device__ __forceinline__ explicit Recip(double y_) {
     y = y_;
     r = __drcp_rn(y_);
-    ok = div_range_ok(y_);
+    const unsigned e = (unsigned)(__double_as_longlong(y_) >> 52) & 0x7ffu;
+    bad = e - 543u > 960u;
   }
   __device__ __forceinline__ Recip(double y_, double r_) {   // r_ = RN(1/y_), y_ in range
     y = y_;
     r = r_;
-    ok = true;
+    bad = false;
   }
-  __device__ __forceinline__ double div(double x) const {
-    const long long bx = __double_as_longlong(x);
-    if (ok && ((unsigned)(bx >> 52) & 0x7ffu) - 543u <= 960u) {
-      const double q = x * r;
-      return fma(fma(-q, y, x), r, q);
-    }
-    if (ok && (bx << 1) == 0) return x * r;
-    return x / y;
+  __device__ __forceinline__ double div(double x) {
+    bad |= !mk_in(x);
+    return mk_div(x, y, r);
   }
+  __device__ __forceinline__ double exact(double x) const { return mk_div(x, y, r); }
 };
 
+struct V9 { double v[NV]; };
+
 // Primitive (src/Flux.c:30-56)
+__device__ __noinline__ V9 primitive_ieee(V9 u) {
+  const double* U = u.v;
+  V9 o;
+  double* P = o.v;
+  const double rho = U[0];
+  const double v1 = U[1] / rho, v2 = U[2] / rho;
+  const double vs = v1 * v1 + v2 * v2;
+  const double th = (2 * U[3] / rho - vs) / 3;
+  const double E = U[3];
+  const double T11 = U[4] / rho - v1 * v1;
+  const double T12 = U[5] / rho - v1 * v2;
+  const double T22 = U[6] / rho - v2 * v2;
+  P[0] = rho; P[1] = v1; P[2] = v2; P[3] = th;
+  P[4] = T11; P[5] = T12; P[6] = T22;
+  P[7] = U[7] - E * v1 - rho * (T11 * v1 + T12 * v2);
+  P[8] = U[8] - E * v2 - rho * (T12 * v1 + T22 * v2);
+  return o;
+}
+
 __device__ __forceinline__ void primitive(const double (&U)[NV], double (&P)[NV]) {
   const double rho = U[0];
-  const Recip R(rho);
-  const Recip third(3.0, 1.0 / 3.0);
+  Recip R(rho);
+  Recip third(3.0, 1.0 / 3.0);
   const double v1 = R.div(U[1]), v2 = R.div(U[2]);
   const double vs = v1 * v1 + v2 * v2;
   const double th = third.div(R.div(2 * U[3]) - vs);
@@ -78,6 +105,14 @@ __device__ __forceinline__ void primitive(const double (&U)[NV], double (&P)[NV]
   P[4] = T11; P[5] = T12; P[6] = T22;
   P[7] = U[7] - E * v1 - rho * (T11 * v1 + T12 * v2);
   P[8] = U[8] - E * v2 - rho * (T12 * v1 + T22 * v2);
+  if (__builtin_expect(R.bad || third.bad, 0)) {
+    V9 u;
+#pragma unroll
+    for (int n = 0; n < NV; n++) u.v[n] = U[n];
+    const V9 o = primitive_ieee(u);
+#pragma unroll
+    for (int n = 0; n < NV; n++) P[n] = o.v[n];
+  }
 }
 
 // moments with an explicit energy (src/Flux.c:65-73, 255-263)
@@ -102,23 +137,27 @@ __device__ __forceinline__ void conservative(const double (&P)[NV], double (&U)[
   moments_e(P[0], P[1], P[2], E, P[4], P[5], P[6], P[7], P[8], U);
 }
 
-// Grad-13 flux along x of a moment vector (src/Flux.c:79-119)
-__device__ __forceinline__ void grad13_flux_x(const double (&U)[NV], double (&F)[NV]) {
+// Grad-13 flux along x of a moment vector (src/Flux.c:79-119).  D: the division
+// policy -- shared reciprocals (fast) or IEEE (cold path).
+template <bool IEEE>
+__device__ __forceinline__ bool grad13_flux_x_t(const double (&U)[NV], double (&F)[NV]) {
   const double rho = U[0];
-  const Recip R(rho);
-  const Recip third(3.0, 1.0 / 3.0);
-  const double v1 = R.div(U[1]), v2 = R.div(U[2]);
+  Recip R(rho);
+  Recip third(3.0, 1.0 / 3.0);
+#define MBM_DIV(D, x) (IEEE ? (x) / D.y : D.div(x))
+  const double v1 = MBM_DIV(R, U[1]), v2 = MBM_DIV(R, U[2]);
   const double vs = v1 * v1 + v2 * v2;
-  const double th = third.div(R.div(2 * U[3]) - vs);
+  const double th = MBM_DIV(third, MBM_DIV(R, 2 * U[3]) - vs);
   const double E = U[3];
-  const double T11 = R.div(U[4]) - v1 * v1;
-  const double T12 = R.div(U[5]) - v1 * v2;
-  const double T22 = R.div(U[6]) - v2 * v2;
+  const double T11 = MBM_DIV(R, U[4]) - v1 * v1;
+  const double T12 = MBM_DIV(R, U[5]) - v1 * v2;
+  const double T22 = MBM_DIV(R, U[6]) - v2 * v2;
   const double q1 = U[7] - E * v1 - rho * (T11 * v1 + T12 * v2);
   const double q2 = U[8] - E * v2 - rho * (T12 * v1 + T22 * v2);
-  const double M111 = R.div(1.2 * q1);
-  const double M121 = R.div(0.4 * q2), M112 = M121;
-  const double M221 = R.div(0.4 * q1), M122 = M221;
+  const double M111 = MBM_DIV(R, 1.2 * q1);
+  const double M121 = MBM_DIV(R, 0.4 * q2), M112 = M121;
+  const double M221 = MBM_DIV(R, 0.4 * q1), M122 = M221;
+#undef MBM_DIV
   const double R11 = 5 * th * th + 7 * th * (T11 - th);
   const double R12 = 7 * th * T12;
   F[0] = rho * v1;
@@ -132,6 +171,29 @@ __device__ __forceinline__ void grad13_flux_x(const double (&U)[NV], double (&F)
          rho * (M111 * v1 + M112 * v2) + 0.5 * rho * (T11 * vs + R11);
   F[8] = q2 * v1 + q1 * v2 + rho * (v1 * v2 * (T11 + T22) + 1.5 * T12 * vs) + E * v1 * v2 +
          rho * (M121 * v1 + M122 * v2) + 0.5 * rho * R12;
+  return IEEE ? false : (R.bad || third.bad);
+}
+
+__device__ __noinline__ V9 grad13_flux_x_ieee(V9 u) {
+  double U[NV], F[NV];
+#pragma unroll
+  for (int n = 0; n < NV; n++) U[n] = u.v[n];
+  grad13_flux_x_t<true>(U, F);
+  V9 o;
+#pragma unroll
+  for (int n = 0; n < NV; n++) o.v[n] = F[n];
+  return o;
+}
+
+__device__ __forceinline__ void grad13_flux_x(const double (&U)[NV], double (&F)[NV]) {
+  if (__builtin_expect(grad13_flux_x_t<false>(U, F), 0)) {
+    V9 u;
+#pragma unroll
+    for (int n = 0; n < NV; n++) u.v[n] = U[n];
+    const V9 o = grad13_flux_x_ieee(u);
+#pragma unroll
+    for (int n = 0; n < NV; n++) F[n] = o.v[n];
+  }
 }
 
 // flux through a face of unit normal (nx, ny): rotate, x-flux, rotate back
@@ -185,12 +247,15 @@ __device__ __forceinline__ double rdamp(double z) {
 template <int FLAG>
 __device__ __forceinline__ double relax(const double (&P)[NV], double (&Out)[NV], double dt,
                                         const Recip& Kn, double F) {
+  // Kn is in the safe range (checked when the kernel starts); the numerator's range
+  // decides between the shared-reciprocal quotient and IEEE division
   const double rho = P[0], th = P[3];
   double v1 = P[1], v2 = P[2];
   double vs = v1 * v1 + v2 * v2;
   double E = 0.5 * rho * vs + 1.5 * rho * th;
   const double nu0 = 1.0;
-  const double coll = Kn.div(nu0 * rho * sqrt(th)) * dt;
+  const double num = nu0 * rho * sqrt(th);
+  const double coll = (__builtin_expect(mk_in(num), 1) ? Kn.exact(num) : div_ieee(num, Kn.y)) * dt;
   if (FLAG == 0 || FLAG == 2) {
     const double g0 = F, g1 = 0.0;
     v1 += dt * g0;
@@ -211,7 +276,8 @@ __device__ __forceinline__ double relax(const double (&P)[NV], double (&Out)[NV]
 template <int FLAG>
 __device__ __forceinline__ double relax_cfl(const double (&P)[NV], double dt, const Recip& Kn) {
   const double nu0 = 1.0;
-  const double coll = Kn.div(nu0 * P[0] * sqrt(P[3])) * dt;
+  const double num = nu0 * P[0] * sqrt(P[3]);
+  const double coll = (__builtin_expect(mk_in(num), 1) ? Kn.exact(num) : div_ieee(num, Kn.y)) * dt;
   return 0.5 * (1 - rdamp<FLAG>(2.0 / 3 * coll));
 }
 
@@ -256,10 +322,17 @@ __device__ __forceinline__ double hll(const double (&PL)[NV], const double (&PR)
   const double lamR = rmax(vR + cR, 0.0);
   const double alph = lamR - lamL;
   if (alph > 0.0) {
-    const Recip A(alph);
+    Recip A(alph);
+    double num[NV];
 #pragma unroll
-    for (int n = 0; n < NV; n++)
-      flx[n] = A.div(lamR * fL[n] - lamL * fR[n] + lamL * lamR * (UR[n] - UL[n]));
+    for (int n = 0; n < NV; n++) {
+      num[n] = lamR * fL[n] - lamL * fR[n] + lamL * lamR * (UR[n] - UL[n]);
+      flx[n] = A.div(num[n]);
+    }
+    if (__builtin_expect(A.bad, 0)) {
+#pragma unroll
+      for (int n = 0; n < NV; n++) flx[n] = div_ieee(num[n], alph);
+    }
   } else {
 #pragma unroll
     for (int n = 0; n < NV; n++) flx[n] = 0.5 * (fL[n] + fR[n]);

@@ -75,7 +75,7 @@ extern "C" int mbm_stage_noalloc(const mbm_block_desc* blocks, int nblocks, cons
   if (!blocks || nblocks < 1 || !in || !out || (heun == 1 && !data0) || (heun != 0 && heun != 1))
     return fail(MBM_EINVAL, "mbm_stage_noalloc: bad argument");
   if (nblocks > NOALLOC_MAX_BLOCKS) return fail(MBM_EINVAL, "mbm_stage_noalloc: more than 64 blocks");
-  if (limiter < 0 || limiter > 4 || !(Kn > 0) || !(dt > 0))
+  if (limiter < 0 || limiter > 4 || !(Kn > 1e-100 && Kn < 1e100) || !(dt > 0))
     return fail(MBM_EINVAL, "mbm_stage_noalloc: bad limiter, Kn or dt");
   cudaStream_t s = (cudaStream_t)stream;
   int dev = 0;
@@ -86,7 +86,8 @@ extern "C" int mbm_stage_noalloc(const mbm_block_desc* blocks, int nblocks, cons
   int nwork = 0;
   for (int b = 0; b < nblocks; b++) {
     const mbm_block_desc& d = blocks[b];
-    if (d.nx < 1 || d.ny < 1 || d.nx > (1 << 20) || d.ny > (1 << 20) || !(d.dx > 0) || !(d.dy > 0))
+    if (d.nx < 1 || d.ny < 1 || d.nx > (1 << 20) || d.ny > (1 << 20) ||
+        !(d.dx > 1e-100 && d.dx < 1e100) || !(d.dy > 1e-100 && d.dy < 1e100))
       return fail(MBM_EINVAL, "mbm_stage_noalloc: bad block extents");
     BlockDev& h = h_blk[b];
     h.nxp = d.nx + 2 * NG;

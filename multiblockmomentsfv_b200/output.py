@@ -126,6 +126,14 @@ class Writer:
     def write(self, layers: Sequence[np.ndarray], t: float, add: int) -> None:
         """layers[b] = L_DATA of block b, (ny+6, nx+6, 9).  add <= 0 starts fresh
         files (STRANDID 1); add > 0 appends with STRANDID add+1."""
+        self._write([zone_payload(U, b.nx, b.ny, self.single) for b, U in zip(self.deck.blocks, layers)], t, add)
+
+    def write_solver(self, solver, t: float, add: int) -> None:
+        """The same from a device solver: the payload is formed on the GPU
+        (mbm_output_fields) and only the output fields cross to the host."""
+        self._write([solver.output_fields(b, self.single).tobytes() for b in range(len(self.deck.blocks))], t, add)
+
+    def _write(self, payloads, t: float, add: int) -> None:
         if self.out_dir:
             os.makedirs(self.out_dir, exist_ok=True)
         fresh = add <= 0
@@ -136,11 +144,11 @@ class Writer:
             if fresh:
                 fh.write(self._manifest())
             esize = 4 if self.single else 8
-            for nb, (b, U) in enumerate(zip(self.deck.blocks, layers)):
+            for nb, (b, payload) in enumerate(zip(self.deck.blocks, payloads)):
                 ni = b.ny + 2
                 nj = b.nx + 2
                 offset = fd.tell()
-                fd.write(zone_payload(U, b.nx, b.ny, self.single))
+                fd.write(payload)
                 nbytes = ni * nj * NVARS_OUT * esize
                 fh.write("ZONE block=%d I=%d J=%d NVARS=%d "
                          "BX=%.16g BY=%.16g DX=%.16g DY=%.16g LFB_I=%d LFB_J=%d "

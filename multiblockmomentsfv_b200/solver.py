@@ -31,7 +31,7 @@ class Solver:
 
     def __init__(self, deck: bf.Deck, scenario: Optional[sc.Scenario] = None, device: int = 0,
                  show_every: int = 20, stream: Optional[int] = None, segment_rows: int = 0,
-                 max_attempts: int = 0):
+                 max_attempts: int = 0, adjoint: bool = False):
         self.deck = deck
         self.scenario = scenario
         self.L = _abi.lib()
@@ -40,6 +40,7 @@ class Solver:
         p.Kn, p.F, p.limiter, p.mode = deck.Kn, deck.F, deck.limiter, _abi.MODE_EXACT
         p.device, p.show_every, p.max_attempts, p.segment_rows = device, show_every, max_attempts, segment_rows
         p.stream = stream
+        p.adjoint = 1 if adjoint else 0
         self._params = p
         ctx = C.c_void_p()
         st = self.L.mbm_create(self._descs, len(deck.blocks), C.byref(p), C.byref(ctx))
@@ -86,6 +87,13 @@ class Solver:
 
     def layers(self, layer: int = L_DATA) -> List[np.ndarray]:
         return [self.download(layer, b) for b in range(len(self.deck.blocks))]
+
+    def output_fields(self, b: int, single: bool = True) -> np.ndarray:
+        """Output's payload of block b computed on the device: ((nx+2)*(ny+2), 10)."""
+        blk = self.deck.blocks[b]
+        a = np.empty(((blk.nx + 2) * (blk.ny + 2), 10), dtype=np.float32 if single else np.float64)
+        self._check(self.L.mbm_output_fields(self.ctx, b, 1 if single else 0, a.ctypes.data))
+        return a
 
     def set_dirichlet(self, b: int, side: int, values: np.ndarray) -> None:
         v = np.ascontiguousarray(values, dtype=np.float64)
@@ -230,16 +238,27 @@ class BatchSolver:
                 self.upload(L_DATA, k, b, sc.initial_block(scn, blk))
         _abi.check(self.L.mbm_set_boundary(self.ctx, L_DATA, 0.0), self.ctx)
 
-    def steps(self, t, tend, max_steps: int = 0, CFLmax: float = 1.0, CFLreg: float = 0.95):
-        """Advance every case; returns (t[], nsteps[], nrej[])."""
+    def steps(self, t, tend, max_steps: int = 0, CFLmax: float = 1.0, CFLreg: float = 0.95,
+              check: bool = True):
+        """Advance every case; returns (t[], nsteps[], nrej[]).  check=False leaves
+        cases that stopped on a non-finite value or the attempt limit to
+        case_status() instead of raising."""
         n = len(self.cases)
         tt = np.ascontiguousarray(np.broadcast_to(np.asarray(t, dtype=np.float64), (n,)).copy())
         te = np.ascontiguousarray(np.broadcast_to(np.asarray(tend, dtype=np.float64), (n,)).copy())
         ns = (C.c_int * n)()
         nr = (C.c_int * n)()
-        _abi.check(self.L.mbm_steps_batch(self.ctx, _dptr(tt), _dptr(te), CFLmax, CFLreg, max_steps, ns, nr),
-                   self.ctx)
+        st = self.L.mbm_steps_batch(self.ctx, _dptr(tt), _dptr(te), CFLmax, CFLreg, max_steps, ns, nr)
+        if check or st not in (_abi.MBM_ENONFINITE, _abi.MBM_ESTEPLIMIT):
+            _abi.check(st, self.ctx)
         return tt, np.array(ns[:]), np.array(nr[:])
+
+    def case_status(self) -> np.ndarray:
+        """Per-case status of the last steps() call (MBM_OK, MBM_ENONFINITE, MBM_ESTEPLIMIT)."""
+        n = len(self.cases)
+        s = (C.c_int * n)()
+        _abi.check(self.L.mbm_case_status(self.ctx, s, n), self.ctx)
+        return np.array(s[:])
 
     def attempts(self) -> int:
         a = C.c_int(0)
@@ -301,7 +320,7 @@ def run(deck: bf.Deck, scenario: sc.Scenario, out_dir: str, single: bool = True,
     w = out.Writer(out_dir, deck, scenario.type_name, single)
     with Solver(deck, scenario, device=device, show_every=show_every) as s:
         s.initialise()
-        w.write(s.layers(), 0.0, -1)
+        w.write_solver(s, 0.0, -1)
         t, nmax = 0.0, 0
         cells = deck.full_grid_size
         for tn in deck.t_out:
@@ -315,7 +334,7 @@ def run(deck: bf.Deck, scenario: sc.Scenario, out_dir: str, single: bool = True,
                 print("   %d steps (%d rejected) to t = %g in %.3f s, %.4f us per cell-update" %
                       (n, rej, t, el, perf))
             nmax += n
-            w.write(s.layers(), t, nmax)
+            w.write_solver(s, t, nmax)
     if verbose:
         print("\n Done after %d steps.\n" % nmax)
     return w, nmax

@@ -125,22 +125,4 @@ def random_deck(rng: np.random.Generator, max_n: int = 12) -> bf.Deck:
     return d
 
 
-def quadrant_deck(n: int, Kn: float = 0.01, limiter: int = bf.LIM_HARMONIC, R13: float = 1.0,
-                  nblocks_side: int = 2) -> bf.Deck:
-    """The scaled square4 layout: blocks of n x n cells tiling [-1,1]^2, all outer
-    edges open (extrapolation), inner edges synchronised."""
-    k = nblocks_side
-    h = 2.0 / k
-    blocks = []
-    for j in range(k):
-        for i in range(k):
-            bid = j * k + i + 1
-            left = bid - 1 if i > 0 else 0
-            right = bid + 1 if i < k - 1 else 0
-            bottom = bid - k if j > 0 else 0
-            top = bid + k if j < k - 1 else 0
-            blocks.append(bf.Block(bid, -1.0 + i * h, -1.0 + (i + 1) * h, -1.0 + j * h,
-                                   -1.0 + (j + 1) * h, n, n, (left, right, bottom, top)))
-    d = bf.Deck(Kn=Kn, R13=R13, limiter=limiter, CFL=0.95)
-    d.blocks = blocks
-    return d
+quadrant_deck = bf.quadrant_deck

@@ -1,0 +1,159 @@
+"""The discrete adjoint (mbm_adjoint_run) against central finite differences of the
+frozen-dt forward map: gradients of J = sum (qx^2 + qy^2) of the final state with
+respect to the initial temperature field and to Kn, in seeded random directions;
+the finite differences come from mbm_replay and, on a small case, from the C
+oracle's own frozen-dt steps; and the torch.autograd.Function over it.
+
+Where the map is smooth (limiters none and average; the HLL wave speeds are smooth
+in subsonic flow) the check holds to 1e-6 at eps = 1e-6.  Minmod, superbee and
+harmonic have kinks (sign changes of the one-sided differences, |d1| = |d2|); the
+adjoint takes the forward branch there (a fixed subgradient), and a finite
+difference of step eps crosses kinks in a fraction of cells that grows with eps,
+so those limiters are checked at eps = 1e-8 with a bound that covers the crossings.
+"""
+import numpy as np
+import pytest
+
+import helpers as H
+from multiblockmomentsfv_b200 import adjoint as adj
+from multiblockmomentsfv_b200 import blockfile as bf
+from multiblockmomentsfv_b200 import output
+from multiblockmomentsfv_b200 import scenario as sc
+from multiblockmomentsfv_b200 import solver as sv
+
+pytestmark = pytest.mark.gpu
+
+
+def _theta0(d, rng):
+    return [1.0 + 0.2 * np.sin(np.linspace(0, 3, b.nx)[None, :] + np.linspace(0, 2, b.ny)[:, None])
+            * rng.uniform(0.5, 1.0) for b in d.blocks]
+
+
+def _fd_check(n, nsteps, every, ndirs, seed, limiter=bf.LIM_AVERAGE, eps=1e-6, Kn=0.01):
+    d = H.quadrant_deck(n, Kn=Kn, limiter=limiter)
+    base = adj.smooth_base(d, seed)
+    rng = np.random.default_rng(seed)
+    th0 = _theta0(d, rng)
+    with adj.Sensitivity(d, base) as S:
+        layers = adj.state_from_theta(d, base, th0)
+        S.load(layers)
+        J, g, gK, dts, ms = S.run(nsteps, every)
+        gth = adj.theta_gradient(d, layers, g)
+        worst = 0.0
+        for _ in range(ndirs):
+            v = [rng.standard_normal(t.shape) for t in th0]
+            S.load(adj.state_from_theta(d, base, [t + eps * w for t, w in zip(th0, v)]))
+            Jp = S.replay(dts)
+            S.load(adj.state_from_theta(d, base, [t - eps * w for t, w in zip(th0, v)]))
+            Jm = S.replay(dts)
+            fd = (Jp - Jm) / (2 * eps)
+            ad = sum(float(np.sum(a * w)) for a, w in zip(gth, v))
+            worst = max(worst, abs(fd - ad) / max(abs(fd), 1e-300))
+        S.load(layers, Kn=Kn * (1 + 1e-6))
+        Jp = S.replay(dts)
+        S.load(layers, Kn=Kn * (1 - 1e-6))
+        Jm = S.replay(dts)
+        fdK = (Jp - Jm) / (2 * Kn * 1e-6)
+        S.load(layers, Kn=Kn)
+        assert abs(S.replay(dts) - J) <= 1e-12 * abs(J)      # replay reproduces the forward run
+    return worst, abs(fdK - gK) / abs(fdK), ms, J
+
+
+@pytest.mark.parametrize("limiter", [bf.LIM_NONE, bf.LIM_AVERAGE])
+def test_adjoint_smooth_limiters(limiter):
+    worst, errK, ms, J = _fd_check(n=24, nsteps=12, every=5, ndirs=6, seed=3, limiter=limiter)
+    assert J > 0
+    assert worst < 1e-6, worst
+    assert errK < 1e-6, errK
+
+
+@pytest.mark.parametrize("limiter", [bf.LIM_MINMOD, bf.LIM_SUPERBEE, bf.LIM_HARMONIC])
+def test_adjoint_kinked_limiters(limiter):
+    worst, errK, ms, J = _fd_check(n=24, nsteps=12, every=5, ndirs=6, seed=3, limiter=limiter, eps=1e-8)
+    assert worst < 1e-3, worst
+    assert errK < 1e-6, errK
+
+
+def test_adjoint_benchmark_case():
+    """4 blocks x 256^2, 200 steps, checkpoints every 20, 16 seeded directions,
+    eps = 1e-6; the adjoint:forward device-time ratio is reported."""
+    worst, errK, ms, J = _fd_check(n=256, nsteps=200, every=20, ndirs=16, seed=11)
+    print(f"adjoint check: worst rel err {worst:.2e}, Kn rel err {errK:.2e}, "
+          f"forward {ms[0]:.1f} ms, adjoint {ms[1]:.1f} ms, ratio {ms[1] / ms[0]:.2f}")
+    assert worst < 1e-6, worst
+    assert errK < 1e-6, errK
+
+
+def _oracle_replay(O, d, layers, dts):
+    """J after the frozen-dt steps of the C oracle (TimeUpdate, then NEW -> DATA)."""
+    o = O.Oracle(d, sc.Scenario.named("riemann2d"))
+    try:
+        for b, U in enumerate(layers):
+            o.set_layer(O.DATA, b, U)
+        o.set_boundary(O.DATA, 0.0)
+        t = 0.0
+        for dt in dts:
+            o.time_update(dt, t)
+            for b in range(len(d.blocks)):
+                o.set_layer(O.DATA, b, o.get_layer(O.NEW, b))
+            t += dt
+        final = o.layers(O.DATA)
+    finally:
+        o.close()
+    J = 0.0
+    for U in final:
+        P = output.primitive(U[bf.NG:-bf.NG, bf.NG:-bf.NG])
+        J += float(np.sum(P[..., 7] ** 2 + P[..., 8] ** 2))
+    return J, final
+
+
+def test_adjoint_against_oracle_differences(oracle_mod):
+    """Directional derivatives from perturbed runs of the C oracle: its frozen-dt
+    states equal the device replay bit for bit, and its central differences match
+    the adjoint."""
+    O = oracle_mod
+    d = H.quadrant_deck(16, Kn=0.01, limiter=bf.LIM_AVERAGE)
+    base = adj.smooth_base(d, 7)
+    rng = np.random.default_rng(7)
+    th0 = _theta0(d, rng)
+    eps = 1e-6
+    with adj.Sensitivity(d, base) as S:
+        layers = adj.state_from_theta(d, base, th0)
+        S.load(layers)
+        J, g, gK, dts, ms = S.run(8, 3)
+        gth = adj.theta_gradient(d, layers, g)
+        S.load(layers)
+        S.replay(dts)
+        dev = [S.s.download(sv.L_DATA, b) for b in range(len(d.blocks))]
+    Jo, final = _oracle_replay(O, d, layers, dts)
+    for b in range(len(d.blocks)):
+        H.assert_bitwise(dev[b][bf.NG:-bf.NG, bf.NG:-bf.NG], final[b][bf.NG:-bf.NG, bf.NG:-bf.NG], f"block {b + 1}")
+    assert abs(Jo - J) <= 1e-13 * abs(J)
+    for _ in range(4):
+        v = [rng.standard_normal(t.shape) for t in th0]
+        Jp, _ = _oracle_replay(O, d, adj.state_from_theta(d, base, [t + eps * w for t, w in zip(th0, v)]), dts)
+        Jm, _ = _oracle_replay(O, d, adj.state_from_theta(d, base, [t - eps * w for t, w in zip(th0, v)]), dts)
+        fd = (Jp - Jm) / (2 * eps)
+        ad = sum(float(np.sum(a * w)) for a, w in zip(gth, v))
+        assert abs(fd - ad) <= 1e-6 * abs(fd), (fd, ad)
+
+
+def test_autograd_function():
+    torch = pytest.importorskip("torch")
+    d = H.quadrant_deck(16, Kn=0.01)
+    base = adj.smooth_base(d, 5)
+    with adj.Sensitivity(d, base) as S:
+        f = adj.make_autograd(S, nsteps=8, every=4)
+        th = torch.ones((4, 16, 16), dtype=torch.float64, requires_grad=True)
+        kn = torch.tensor(0.01, dtype=torch.float64, requires_grad=True)
+        J = f(th, kn)
+        J.backward()
+        assert th.grad.shape == th.shape and torch.isfinite(th.grad).all()
+        assert kn.grad is not None and torch.isfinite(kn.grad)
+        # the gradient is the one mbm_adjoint_run returns for the same state
+        layers = adj.state_from_theta(d, base, list(th.detach().numpy()))
+        S.load(layers, 0.01)
+        _, g, gK, _, _ = S.run(8, 4)
+        ref = np.stack(adj.theta_gradient(d, layers, g))
+        assert np.allclose(th.grad.numpy(), ref, rtol=1e-12, atol=0)
+        assert abs(float(kn.grad) - gK) <= 1e-12 * abs(gK)

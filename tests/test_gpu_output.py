@@ -1,0 +1,85 @@
+"""Output staged on the device (mbm_output_fields) against the host-side payload of
+the downloaded state, and failure detection: a NaN in the state ends mbm_steps with
+MBM_ENONFINITE instead of running on."""
+import os
+
+import numpy as np
+import pytest
+
+import helpers as H
+from multiblockmomentsfv_b200 import _abi, output, solver
+from multiblockmomentsfv_b200 import scenario as sc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("single", [True, False])
+def test_output_fields_equal_host_payload(single):
+    d = H.random_deck(np.random.default_rng(7))
+    with solver.Solver(d, sc.Scenario.named("riemann2d")) as s:
+        s.initialise()
+        s.steps(0.0, 0.02)
+        for b, blk in enumerate(d.blocks):
+            host = output.zone_payload(s.download(solver.L_DATA, b), blk.nx, blk.ny, single)
+            dev = s.output_fields(b, single).tobytes()
+            assert dev == host, f"block {b + 1}"
+
+
+def test_writer_from_device_writes_identical_files(tmp_path):
+    d = H.quadrant_deck(40, Kn=0.01, limiter=2)
+    with solver.Solver(d, sc.Scenario.seeded_quadrant(4)) as s:
+        s.initialise()
+        w_host = output.Writer(str(tmp_path / "host"), d, "Quadrant")
+        w_dev = output.Writer(str(tmp_path / "dev"), d, "Quadrant")
+        t = 0.0
+        for k, tend in enumerate([0.01, 0.02]):
+            t, _, _ = s.steps(t, tend)
+            w_host.write(s.layers(), t, k)
+            w_dev.write_solver(s, t, k)
+    with open(w_host.dat, "rb") as a, open(w_dev.dat, "rb") as b:
+        assert a.read() == b.read()
+    ok, mx, msg = output.compare(w_dev.base, w_host.base, 0.0, 0.0)
+    assert ok and mx == 0.0, msg
+
+
+def test_nan_in_state_is_reported():
+    d = H.quadrant_deck(32, Kn=0.01)
+    with solver.Solver(d, sc.Scenario.seeded_quadrant(2)) as s:
+        s.initialise()
+        U = s.download(solver.L_DATA, 1)
+        U[10, 12, 3] = np.nan
+        s.upload(solver.L_DATA, 1, U)
+        with pytest.raises(_abi.MBMError) as e:
+            s.steps(0.0, 0.05)
+        assert e.value.status == _abi.MBM_ENONFINITE
+        # the context stays usable: a clean state steps again
+        s.initialise()
+        t, n, _ = s.steps(0.0, 0.01)
+        assert n > 0 and abs(t - 0.01) < 1e-15
+
+
+def test_batch_nonfinite_case_stops_alone():
+    """In a batch, a case that goes non-finite stops with MBM_ENONFINITE while the
+    others run to the end with the results they have alone."""
+    cases = [(H.quadrant_deck(24, Kn=0.01), sc.Scenario.seeded_quadrant(k)) for k in range(3)]
+    with solver.BatchSolver(cases) as bs:
+        bs.initialise()
+        U = bs.download(solver.L_DATA, 1, 2)
+        U[8, 9, 0] = np.inf
+        bs.upload(solver.L_DATA, 1, 2, U)
+        with pytest.raises(_abi.MBMError) as e:
+            bs.steps(0.0, 0.02)
+        assert e.value.status == _abi.MBM_ENONFINITE
+        bs.initialise()
+        bs.upload(solver.L_DATA, 1, 2, U)
+        t, ns, _ = bs.steps(0.0, 0.02, check=False)
+        st = bs.case_status()
+        assert list(st) == [_abi.MBM_OK, _abi.MBM_ENONFINITE, _abi.MBM_OK]
+        assert ns[1] == 0 and abs(t[0] - 0.02) < 1e-15 and abs(t[2] - 0.02) < 1e-15
+        ref = [bs.download(solver.L_DATA, k, b) for k in (0, 2) for b in range(4)]
+    for i, k in enumerate((0, 2)):
+        with solver.Solver(cases[k][0], cases[k][1]) as s:
+            s.initialise()
+            s.steps(0.0, 0.02)
+            for b in range(4):
+                H.assert_bitwise(s.download(solver.L_DATA, b), ref[4 * i + b], f"case {k} block {b + 1}")

@@ -82,6 +82,8 @@ def test_ghost_map_rejects_bad_tables():
         solver.ghost_map([B(1, 0, 1, 0, 1, 5, 5, (0, 2, 0, 0)), B(2, 1, 2, 0, 1, 5, 6, (1, 0, 0, 0))])
     with pytest.raises(_abi.MBMError):      # too narrow: a ghost cell keeps no defined source
         solver.ghost_map([B(1, 0, 1, 0, 1, 1, 5, (-1, -1, 0, 0))])
+    with pytest.raises(_abi.MBMError):      # cell size outside (1e-100, 1e100)
+        solver.ghost_map([B(1, 0, 1e-200, 0, 1, 5, 5, (-1, -1, 0, 0))])
 
 
 def test_dirichlet_edge_order():
