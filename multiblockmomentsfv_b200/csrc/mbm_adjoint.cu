@@ -83,7 +83,9 @@ __device__ __forceinline__ double slope_at(const AdjArgs& a, const BlockDev& B, 
 }
 
 // pass B: faces (I,J)|(I+1,J) (dir 1) or (I,J)|(I,J+1) (dir 2) next to an output cell
-__global__ void adj_faces(AdjArgs a, long long ncell, int dir) {
+// 128 registers: four 128-thread CTAs per SM hide the neighbour loads better than
+// the spill-free allocation at half the occupancy
+__global__ void __launch_bounds__(128, 4) adj_faces(AdjArgs a, long long ncell, int dir) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, J;
   if (k >= ncell || !locate(a.blk, a.nblk, k, b, I, J)) return;
@@ -121,42 +123,54 @@ __global__ void adj_faces(AdjArgs a, long long ncell, int dir) {
   }
 }
 
-// adjoint of the reconstruction and slopes along one direction, accumulated into Pb
+// adjoint of the reconstruction and slopes along one direction, accumulated into Pb;
+// called for cells off the outermost ring (1 <= c <= n-2).  All loads of one
+// component are issued before any arithmetic; the slope terms of a neighbour are
+// skipped when its slope adjoint is zero (cells no output depends on may hold no
+// state, and 0 * NaN would leak into the sum)
 __device__ __forceinline__ void gather_dir(const AdjArgs& a, const BlockDev& B, int I, int J, int dir,
                                            const double* FL, const double* FR, double* Pb) {
   const long long s = dir == 1 ? 1 : B.pitch;
   const int n = dir == 1 ? B.nxp : B.nyp, c = dir == 1 ? I : J;
   const double h = dir == 1 ? B.dx : B.dy;
   const long long i0 = cidx(B, I, J);
+  const bool lft = c >= 2, rgt = c <= n - 3;      // slopes of c-1 and c+1 exist (off the ring)
+#pragma unroll 1
   for (int m = 0; m < NV; m++) {
     const long long i = i0 + m * B.plane;
-    auto fl = [&](int off) { const int q = c + off; return (q >= 0 && q < n) ? FL[i + off * s] : 0.0; };
-    auto fr = [&](int off) { const int q = c + off; return (q >= 0 && q < n) ? FR[i + off * s] : 0.0; };
-    auto lam_s = [&](int off) { return 0.5 * h * (fl(off) - fr(off - 1)); };   // adjoint of S(c+off)
+    // face (q | q+1) adjoints: FL = its left state, FR = its right state
+    const double flm = FL[i - s], fl0 = FL[i], flp = FL[i + s];
+    const double frm2 = lft ? FR[i - 2 * s] : 0.0, frm = FR[i - s], fr0 = FR[i];
+    const double pm2 = lft ? a.P[i - 2 * s] : 0.0, pm = a.P[i - s], p0 = a.P[i], pp = a.P[i + s];
+    const double pp2 = rgt ? a.P[i + 2 * s] : 0.0;
     // direct: left state of face c|c+1, right state of face c-1|c
-    double g = fl(0) + fr(-1);
-    // through the slopes of c-1, c, c+1 (each on the cells it reads)
-    for (int off = -1; off <= 1; off++) {
-      const int q = c + off;
-      if (q < 1 || q > n - 2) continue;
-      const double lsv = lam_s(off);
-      if (lsv == 0.0) continue;
-      const long long iq = i + off * s;
-      const double d1 = a.P[iq] - a.P[iq - s], d2 = a.P[iq + s] - a.P[iq];
+    double g = fl0 + frm;
+    // S(q) = L(P(q)-P(q-1), P(q+1)-P(q)) / h, its adjoint h/2 (FL(q) - FR(q-1))
+    const double l0 = 0.5 * h * (fl0 - frm);
+    if (l0 != 0.0) {
       double g1, g2;
-      mbm_adj::limit_grad(a.limiter, d1, d2, &g1, &g2);
-      // S(q) = L(P(q)-P(q-1), P(q+1)-P(q)) / h
-      if (off == 0) g += lsv * (g1 - g2) / h;
-      if (off == -1) g += lsv * g2 / h;
-      if (off == 1) g -= lsv * g1 / h;
+      mbm_adj::limit_grad(a.limiter, p0 - pm, pp - p0, &g1, &g2);
+      g += l0 * (g1 - g2) / h;
+    }
+    const double lm = lft ? 0.5 * h * (flm - frm2) : 0.0;
+    if (lm != 0.0) {
+      double g1, g2;
+      mbm_adj::limit_grad(a.limiter, pm - pm2, p0 - pm, &g1, &g2);
+      g += lm * g2 / h;
+    }
+    const double lp = rgt ? 0.5 * h * (flp - fr0) : 0.0;
+    if (lp != 0.0) {
+      double g1, g2;
+      mbm_adj::limit_grad(a.limiter, pp - p0, pp2 - pp, &g1, &g2);
+      g -= lp * g1 / h;
     }
     Pb[m] += g;
   }
 }
 
 // pass C: per cell, back to the stage input (and Data0)
-__global__ void adj_cells(AdjArgs a, long long ncell, const double* FLx, const double* FRx, const double* FLy,
-                          const double* FRy) {
+__global__ void __launch_bounds__(128, 4) adj_cells(AdjArgs a, long long ncell, const double* FLx,
+                                                    const double* FRx, const double* FLy, const double* FRy) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, J;
   if (k >= ncell || !locate(a.blk, a.nblk, k, b, I, J)) return;
@@ -214,28 +228,31 @@ __global__ void adj_cells(AdjArgs a, long long ncell, const double* FLx, const d
   if ((threadIdx.x & 31) == 0 && knb != 0.0) atomicAdd(a.knb, knb);
 }
 
-// adjoint of the ghost fill: ghost adjoint -> its source cell (wall signs), then zero
+// adjoint of the ghost fill: ghost adjoint -> its source cell (wall signs), then
+// zero; one thread per (ghost cell, component)
 __global__ void adj_ghosts(const BlockDev* __restrict__ blk, const GhostEntry* __restrict__ map, int n, double* l) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * NV) return;
+  const int i = (int)(t / NV), m = (int)(t - (long long)i * NV);
   const GhostEntry e = map[i];
   const BlockDev D = blk[e.dst_blk];
+  double* g = l + D.off + e.dst + m * D.plane;
+  const double v = *g;
+  *g = 0.0;
+  if (e.src < 0 || v == 0.0) return;          // Dirichlet ghosts have no source
   const int sblk = e.src_blk_flags & 0xffff;
   const bool fx = (e.src_blk_flags >> 16) & 1, fy = (e.src_blk_flags >> 17) & 1;
-  for (int m = 0; m < NV; m++) {
-    double* g = l + D.off + e.dst + m * D.plane;
-    const double v = *g;
-    *g = 0.0;
-    if (e.src < 0 || v == 0.0) continue;       // Dirichlet ghosts have no source
-    const BlockDev S = blk[sblk];
-    const bool flip = (fx && (m == 1 || m == 5 || m == 7)) != (fy && (m == 2 || m == 5 || m == 8));
-    atomicAdd(l + S.off + e.src + m * S.plane, flip ? -v : v);
-  }
+  const BlockDev S = blk[sblk];
+  const bool flip = (fx && (m == 1 || m == 5 || m == 7)) != (fy && (m == 2 || m == 5 || m == 8));
+  atomicAdd(l + S.off + e.src + m * S.plane, flip ? -v : v);
 }
 
-// dJ/dU of J = sum over interior cells of q1^2 + q2^2 (heat flux of the final state)
+// dJ/dU of J = sum over interior cells of q1^2 + q2^2 (heat flux of the final state);
+// each CTA writes its partial sum (fixed order: warp shuffles, then the warps in
+// order), so J does not depend on scheduling and finite differences of it are clean
 __global__ void adj_functional(const BlockDev* __restrict__ blk, int nblk, const double* x, double* l,
-                               long long ncell, double* J) {
+                               long long ncell, double* part) {
+  __shared__ double ws[4];
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, Jj;
   double jv = 0.0;
@@ -255,7 +272,25 @@ __global__ void adj_functional(const BlockDev* __restrict__ blk, int nblk, const
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) jv += __shfl_xor_sync(0xffffffffu, jv, o);
-  if ((threadIdx.x & 31) == 0 && jv != 0.0) atomicAdd(J, jv);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = jv;
+  __syncthreads();
+  if (threadIdx.x == 0) part[blockIdx.x] = ((ws[0] + ws[1]) + ws[2]) + ws[3];
+}
+
+// J = the partial sums added in a fixed order by one CTA
+__global__ void sum_partials(const double* part, int n, double* J) {
+  __shared__ double ws[8];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += part[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; w++) t += ws[w];
+    *J = t;
+  }
 }
 
 cudaError_t adjoint_stage(const AdjArgs& a0, long long ncell, double* FLx, double* FRx, double* FLy,
@@ -274,13 +309,16 @@ cudaError_t adjoint_stage(const AdjArgs& a0, long long ncell, double* FLx, doubl
 
 cudaError_t adjoint_ghosts(const BlockDev* blk, const GhostEntry* map, int n, double* l, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  adj_ghosts<<<(n + 127) / 128, 128, 0, s>>>(blk, map, n, l);
+  adj_ghosts<<<(unsigned)(((long long)n * NV + 255) / 256), 256, 0, s>>>(blk, map, n, l);
   return cudaGetLastError();
 }
 
+// part: (ncell + 127) / 128 doubles of scratch
 cudaError_t adjoint_functional(const BlockDev* blk, int nblk, const double* x, double* l, long long ncell,
-                               double* J, cudaStream_t s) {
-  adj_functional<<<(unsigned)((ncell + 127) / 128), 128, 0, s>>>(blk, nblk, x, l, ncell, J);
+                               double* part, double* J, cudaStream_t s) {
+  const unsigned G = (unsigned)((ncell + 127) / 128);
+  adj_functional<<<G, 128, 0, s>>>(blk, nblk, x, l, ncell, part);
+  sum_partials<<<1, 256, 0, s>>>(part, (int)G, J);
   return cudaGetLastError();
 }
 

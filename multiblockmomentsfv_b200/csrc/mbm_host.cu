@@ -32,7 +32,7 @@ cudaError_t adjoint_stage(const AdjArgs& a0, long long ncell, double* FLx, doubl
                           double* FRy, cudaStream_t s);
 cudaError_t adjoint_ghosts(const BlockDev* blk, const GhostEntry* map, int n, double* l, cudaStream_t s);
 cudaError_t adjoint_functional(const BlockDev* blk, int nblk, const double* x, double* l, long long ncell,
-                               double* J, cudaStream_t s);
+                               double* part, double* J, cudaStream_t s);
 cudaError_t launch_fill_uniform(double* base, long long plane, cudaStream_t s);
 cudaError_t launch_stage_cfl(const BlockDev* blk, int nblk, const CaseDev* cases,
                              unsigned long long* lam, int stage, double* out, cudaStream_t s);
@@ -99,6 +99,7 @@ struct mbm_ctx {
   double* adj_dtlog = nullptr;
   double* adj_scal = nullptr;       // [0] dJ/dKn, [1] J
   double* adj_dtrep = nullptr;      // dt values of mbm_replay
+  double* adj_part = nullptr;       // per-CTA partial sums of J
   int adj_nsteps = 0, adj_every = 0, adj_nrep = 0;
   std::string err;
 };
@@ -648,6 +649,7 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   cudaFree(c->adj_segT);
   cudaFree(c->adj_dtlog);
   cudaFree(c->adj_dtrep);
+  cudaFree(c->adj_part);
   cudaFree(c->adj_scal);
   cudaFree(c->dtrace);
   cudaFree(c->dcfl);
@@ -922,10 +924,17 @@ extern "C" int mbm_trace_case(mbm_ctx* c, int k, double* rec, int cap, int* n) {
 // Discrete adjoint of a Steps run (hand-written reverse of Update and SetBoundary,
 // mbm_adjoint.cu), dt frozen from the forward run, checkpoints every k steps.
 
+static long long ncells(mbm_ctx* c) {
+  long long n = 0;
+  for (auto& d : c->hblk) n += (long long)d.nxp * d.nyp;
+  return n;
+}
+
 static int adj_alloc(mbm_ctx* c, int nsteps, int every) {
   if (!c->adj_buf[0])
     for (int k = 0; k < 8; k++) CK(cudaMalloc(&c->adj_buf[k], sizeof(double) * c->layer_elems));
   if (!c->adj_scal) CK(cudaMalloc(&c->adj_scal, sizeof(double) * 2));
+  if (!c->adj_part) CK(cudaMalloc(&c->adj_part, sizeof(double) * ((ncells(c) + 127) / 128)));
   if (nsteps > c->adj_nsteps || every != c->adj_every) {
     cudaFree(c->adj_ckpt);
     cudaFree(c->adj_seg);
@@ -967,11 +976,6 @@ static int frozen_step(mbm_ctx* c, const double* in, double* out, const double* 
   return MBM_OK;
 }
 
-static long long ncells(mbm_ctx* c) {
-  long long n = 0;
-  for (auto& d : c->hblk) n += (long long)d.nxp * d.nyp;
-  return n;
-}
 
 // reverse of one step: lam (adjoint of D_{n+1}, interior) -> lam_next (adjoint of
 // D_n); Tn = stage 1 of D_n with its ghost fill
@@ -1052,7 +1056,7 @@ extern "C" int mbm_adjoint_run(mbm_ctx* c, double* t, int nsteps, int every, dou
   double* lam2 = c->adj_buf[1];
   CK(cudaMemsetAsync(c->adj_scal, 0, sizeof(double) * 2, c->stream));
   CK(cudaMemsetAsync(lam, 0, bytes, c->stream));
-  CK(adjoint_functional(c->dblk, c->nblk, c->buf[h.cur], lam, ncells(c), c->adj_scal + 1, c->stream));
+  CK(adjoint_functional(c->dblk, c->nblk, c->buf[h.cur], lam, ncells(c), c->adj_part, c->adj_scal + 1, c->stream));
   // reverse sweep over segments [s*every, min((s+1)*every, n))
   const int cur0 = h.cur;
   if ((st = frozen_begin(c))) return st;
@@ -1132,8 +1136,10 @@ extern "C" int mbm_replay(mbm_ctx* c, const double* dts, int n, double* J) {
   if (J) {
     if (!c->adj_buf[0]) CK(cudaMalloc(&c->adj_buf[0], sizeof(double) * c->layer_elems));
     if (!c->adj_scal) CK(cudaMalloc(&c->adj_scal, sizeof(double) * 2));
+    if (!c->adj_part) CK(cudaMalloc(&c->adj_part, sizeof(double) * ((ncells(c) + 127) / 128)));
     CK(cudaMemsetAsync(c->adj_scal, 0, sizeof(double) * 2, c->stream));
-    CK(adjoint_functional(c->dblk, c->nblk, c->buf[cur], c->adj_buf[0], ncells(c), c->adj_scal + 1, c->stream));
+    CK(adjoint_functional(c->dblk, c->nblk, c->buf[cur], c->adj_buf[0], ncells(c), c->adj_part, c->adj_scal + 1,
+                          c->stream));
     double sc[2];
     CK(cudaMemcpyAsync(sc, c->adj_scal, sizeof sc, cudaMemcpyDeviceToHost, c->stream));
     if ((st = wait_stream(c))) return st;
