@@ -10,6 +10,12 @@ accepted Heun step (two stages, two ghost fills, the dt controller); cell-update
 src/Main.c:223).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--mode fast|exact]
+
+The headline runs the stage kernel in fast arithmetic (MBM_MODE_FAST: multiply-add
+contraction, reciprocal-multiply quotients; tests/test_gpu_fast.py holds it within
+1e-10 of the reference per field after one step and 1e-8 at t = 0.3 on this
+workload); the line also carries the bitwise mode's figures under "exact_mode".
 
 Prints one JSON line on rank 0.  Under torchrun each rank advances its own
 replica of the workload (weak scaling, no collective on the data path); the
@@ -152,7 +158,7 @@ def batched_leg(a, local, stream, rank):
     cases = sv.batch_workload(seed=a.seed + rank, ncases=a.batch_cases)
     cells = [d.full_grid_size for d, _ in cases]
     ev = lambda: torch.cuda.Event(enable_timing=True)
-    with sv.BatchSolver(cases, device=local, stream=stream.cuda_stream) as bs:
+    with sv.BatchSolver(cases, device=local, stream=stream.cuda_stream, mode=a.mode) as bs:
         bs.initialise()
         bs.steps(0.0, 10.0, max_steps=2, check=False)
         bs.initialise()
@@ -167,7 +173,7 @@ def batched_leg(a, local, stream, rank):
     upd_b = float(sum(c * n for c, n in zip(cells, ns)))
     ms_s, upd_s, ns_serial = 0.0, 0.0, []
     for (d, scn), c in zip(cases, cells):
-        with sv.BatchSolver([(d, scn)], device=local, stream=stream.cuda_stream) as s1:
+        with sv.BatchSolver([(d, scn)], device=local, stream=stream.cuda_stream, mode=a.mode) as s1:
             s1.initialise()
             s1.steps(0.0, 10.0, max_steps=2, check=False)
             s1.initialise()
@@ -193,6 +199,28 @@ def batched_leg(a, local, stream, rank):
                         "Steps loop each"}
 
 
+def exact_leg(a, d, scn, local, stream):
+    """The same workload in the bitwise mode (MBM_MODE_EXACT, bit for bit the
+    reference): cell-updates/s of a shorter step loop and the stage kernels alone."""
+    import torch
+    from multiblockmomentsfv_b200 import solver as sv
+    with sv.Solver(d, scn, device=local, show_every=0, stream=stream.cuda_stream,
+                   segment_rows=a.segment_rows, mode="exact") as s:
+        s.initialise()
+        t, _, _ = s.steps(0.0, 0.3, max_steps=a.warmup)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t, n, _ = s.steps(t, 0.3, max_steps=a.exact_steps)
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1)
+        ms1, ms2 = s.time_stage(0, 1e-4, reps=5), s.time_stage(1, 1e-4, reps=5)
+    return {"value": d.full_grid_size * n / (ms / 1e3), "unit": "cell-updates/s", "steps": n,
+            "ms_per_step": ms / max(1, n), "ms_per_launch": [ms1, ms2],
+            "roofline_frac": BYTES_PER_CELL_UPDATE * d.full_grid_size / ((ms1 + ms2) / 1e3) / 1e9
+                             / measured_peaks()[0]}
+
+
 def adjoint_leg(a, local, stream):
     """The discrete adjoint: J = sum(qx^2 + qy^2) after N Heun steps on 4 blocks of
     n x n cells, gradient wrt the initial temperature field and Kn, checkpoints every
@@ -205,7 +233,7 @@ def adjoint_leg(a, local, stream):
     d = bf.quadrant_deck(n, Kn=0.01)
     base = adj.smooth_base(d, a.seed)
     th0 = [np.ones((b.ny, b.nx)) for b in d.blocks]
-    with adj.Sensitivity(d, base, device=local, stream=stream.cuda_stream) as S:
+    with adj.Sensitivity(d, base, device=local, stream=stream.cuda_stream, mode=a.mode) as S:
         layers = adj.state_from_theta(d, base, th0)
         S.load(layers)
         S.run(min(nsteps, 2 * every), every)          # warm-up
@@ -233,6 +261,10 @@ def main():
     ap.add_argument("--adjoint-n", type=int, default=256, help="cells per block side in the adjoint leg (0 = skip)")
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--adjoint-every", type=int, default=20)
+    ap.add_argument("--mode", default="fast", choices=["fast", "exact"],
+                    help="stage-kernel arithmetic: fast (within 1e-10 / 1e-8 of the reference) or exact (bitwise)")
+    ap.add_argument("--exact-steps", type=int, default=100,
+                    help="steps of the bitwise-mode comparison line when --mode fast (0 = skip)")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3
@@ -260,7 +292,7 @@ def main():
     cells = d.full_grid_size
     stream = torch.cuda.Stream()
     s = sv.Solver(d, scn, device=local, show_every=0, stream=stream.cuda_stream,
-                  segment_rows=a.segment_rows)
+                  segment_rows=a.segment_rows, mode=a.mode)
     s.initialise()
     t, n0, _ = s.steps(0.0, 0.3, max_steps=a.warmup)
 
@@ -334,6 +366,7 @@ def main():
     e2e_value = world * cells * e2e_steps / (ms_e2e / 1e3)
 
     s.close()
+    exact = exact_leg(a, d, scn, local, stream) if (a.mode == "fast" and a.exact_steps > 0) else None
     batched = batched_leg(a, local, stream, rank) if a.batch_cases > 0 else None
     adjoint = adjoint_leg(a, local, stream) if a.adjoint_n > 0 else None
 
@@ -355,8 +388,10 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": f"synthetic: seeded quadrant state (seed {a.seed}+rank)",
             "config": {"workload": f"scaled square4: 4 blocks x {a.n}^2 cells ({cells} cells), open outer "
-                                   "edges, Kn=0.01, R13=1, harmonic, CFL 0.95, FP64, bitwise mode",
-                       "cells": cells, "rejected_attempts": nrej,
+                                   "edges, Kn=0.01, R13=1, harmonic, CFL 0.95, FP64, "
+                                   + ("fast mode (within 1e-10 of the reference after one step, 1e-8 at t_end; "
+                                      "measured 5e-13 at t=0.3)" if a.mode == "fast" else "bitwise mode"),
+                       "mode": a.mode, "cells": cells, "rejected_attempts": nrej,
                        "l2": "working set 3 layers x 4 blocks x 9 planes = "
                              f"{3 * 9 * 8 * sum(b.cells for b in d.blocks) / 1e6:.0f} MB > 126 MB L2, no flush",
                        "parallelism": f"replicas x{world}", "launch": launch},
@@ -374,6 +409,7 @@ def main():
             "cpu_baseline": cpu,
             "batched": batched,
             "adjoint": adjoint,
+            "exact_mode": exact,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -44,6 +44,9 @@ extern "C" {
 
 /* arithmetic modes */
 #define MBM_MODE_EXACT 0   /* operation-for-operation the reference: bitwise-equal results */
+#define MBM_MODE_FAST  1   /* multiply-add contraction and reciprocal-multiply quotients in the
+                              stage kernel: within 1e-10 relative per field of the reference
+                              after one step and 1e-8 at the end time (not bitwise) */
 
 /* One block: the DB_Block fields the path reads (src/defs.h:59-68). */
 typedef struct {

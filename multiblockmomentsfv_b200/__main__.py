@@ -2,14 +2,16 @@
 
     python -m multiblockmomentsfv_b200 -bfile cases/squareSmall.txt -out runs/ss [-double]
         [-refine n] [-CFL x] [-Kn x] [-R13 x] [-limiter name] [-sfile file]
-        [-scenario riemann2d|ffs|quadrant:SEED|uniform:r,u,v,th] [-device k]
+        [-scenario riemann2d|ffs|quadrant:SEED|uniform:r,u,v,th] [-device k] [-fast]
 
 Flags keep the reference's meaning and its quirks: numeric overrides pass through
 ``float`` (src/tools.c:38-46), -refine precedes the block file, and -sfile reloads the
 first zones of a result pair into L_DATA with the reference's mapping of the stored
 fields (src/Mesh.c:391-476: the stored pressure p goes where the temperature belongs and
 P_ij where T_ij belongs).  -scenario picks the initial/Dirichlet state that the
-reference hard-codes in src/Scenario.c (default riemann2d).
+reference hard-codes in src/Scenario.c (default riemann2d).  -fast runs the stage
+kernel in fast arithmetic (MBM_MODE_FAST: within 1e-10 of the reference per field after
+one step, 1e-8 at the end time, not bitwise).
 """
 from __future__ import annotations
 
@@ -86,7 +88,8 @@ def main(argv=None) -> int:
           (deck.Kn, deck.R13, deck.CFL, bf.limiter_name(deck.limiter), _arg(argv, "-bfile", "blockfile.txt")))
     w = out.Writer(out_dir, deck, scn.type_name, single)
     sfile = _arg(argv, "-sfile")
-    with sv.Solver(deck, scn, device=device) as s:
+    mode = "fast" if "-fast" in argv else "exact"
+    with sv.Solver(deck, scn, device=device, mode=mode) as s:
         if sfile:
             for b, U in enumerate(load_restart(deck, sfile)):
                 s.upload(sv.L_DATA, b, U)

@@ -13,6 +13,8 @@ from . import build as _build
 MBM_OK, MBM_EINVAL, MBM_ENONFINITE, MBM_ETIMEOUT, MBM_ECUDA, MBM_ENOMEM, MBM_ESTEPLIMIT, MBM_ENODEV = range(8)
 L_DATA, L_TMP, L_NEW = 0, 1, 2
 MODE_EXACT = 0
+MODE_FAST = 1
+MODES = {"exact": MODE_EXACT, "fast": MODE_FAST}
 
 # every symbol include/mbm_b200.h declares
 EXPORTS = (

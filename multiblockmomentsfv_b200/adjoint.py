@@ -85,10 +85,10 @@ class Sensitivity:
     density and velocity of the initial states (padded moment layers)."""
 
     def __init__(self, deck: bf.Deck, base: Sequence[np.ndarray], device: int = 0, stream=None,
-                 scenario: Optional[sc.Scenario] = None):
+                 scenario: Optional[sc.Scenario] = None, mode: str = "exact"):
         self.deck = deck
         self.base = list(base)
-        self.s = sv.Solver(deck, scenario, device=device, show_every=0, stream=stream, adjoint=True)
+        self.s = sv.Solver(deck, scenario, device=device, show_every=0, stream=stream, adjoint=True, mode=mode)
         self.L = _bind(self.s.L)
 
     def close(self):

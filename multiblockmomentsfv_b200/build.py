@@ -2,8 +2,9 @@
 
 sm_100a only.  -fmad=false keeps every multiply and add of the forward path
 separately rounded (the bitwise mode depends on it); double division and sqrt are
-IEEE by default.  The adjoint kernels are derivatives, not restatements of the
-reference's arithmetic, and are compiled with fused multiply-adds.
+IEEE by default.  The adjoint kernels (derivatives, not restatements of the
+reference's arithmetic) and the fast-arithmetic stage kernel are compiled with
+fused multiply-adds.
 """
 from __future__ import annotations
 
@@ -16,15 +17,15 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libmbm_b200.so")
 
-SOURCES = ["mbm_host.cu", "mbm_kernels.cu", "mbm_noalloc.cu", "mbm_adjoint.cu"]
-HEADERS = ["mbm_internal.h", "mbm_math.cuh", "mbm_adjoint_math.cuh"]
+SOURCES = ["mbm_host.cu", "mbm_kernels.cu", "mbm_stage_fast.cu", "mbm_noalloc.cu", "mbm_adjoint.cu"]
+HEADERS = ["mbm_internal.h", "mbm_math.cuh", "mbm_stage.cuh", "mbm_adjoint_math.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
     "-Xcompiler", "-fPIC",
 ]
-FMAD = {"mbm_adjoint.cu": "true"}          # every other source: -fmad=false
+FMAD = {"mbm_adjoint.cu": "true", "mbm_stage_fast.cu": "true"}   # every other source: -fmad=false
 
 
 def nvcc() -> str:

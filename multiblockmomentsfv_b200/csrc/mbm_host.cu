@@ -19,13 +19,19 @@
 #include "mbm_internal.h"
 
 namespace mbm {
+namespace bitwise {
 cudaError_t launch_stage(int lim, const StageArgs& a, int grid, cudaStream_t s);
+int stage_ctas_per_sm();
+}
+namespace fastmath {
+cudaError_t launch_stage(int lim, const StageArgs& a, int grid, cudaStream_t s);
+int stage_ctas_per_sm();
+}
 cudaError_t launch_ghost(const BlockDev* blk, const CaseDev* cases, const GhostEntry* map, int n,
                          double* const buf[3], const double* dirichlet, int sel, cudaStream_t s);
 cudaError_t launch_control(CaseDev* cases, int ncases, const BlockDev* blk, unsigned long long* lam,
                            double* trace, int* queues, cudaGraphConditionalHandle h, int use_handle,
                            cudaStream_t s);
-int stage_ctas_per_sm();
 cudaError_t launch_ckpt(const CaseDev* cases, const double* buf0, const double* buf1, long long layer_elems,
                         int grid, cudaStream_t s);
 cudaError_t adjoint_stage(const AdjArgs& a0, long long ncell, double* FLx, double* FRx, double* FLy,
@@ -91,6 +97,7 @@ struct mbm_ctx {
   cudaGraphExec_t gexec = nullptr;
   bool host_loop = false;           // MBM_HOST_LOOP=1: drive the step loop from the host
   bool adjoint = false;             // graph body records checkpoints and dt (mbm_params.adjoint)
+  bool fast = false;                // MBM_MODE_FAST: the fastmath stage kernel
   // adjoint work space (allocated on first use)
   double* adj_buf[8] = {nullptr};   // two adjoint layers, primitives, 4 face-adjoint layers, spare
   double* adj_ckpt = nullptr;
@@ -330,7 +337,8 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
     a.queue = c->dqueue + heun * 5 + g.lim;
     a.sel_in = sel_in; a.sel_d0 = sel_d0; a.sel_out = sel_out;
     a.heun = heun;
-    cudaError_t e = launch_stage(g.lim, a, g.grid, c->stream);
+    cudaError_t e = c->fast ? fastmath::launch_stage(g.lim, a, g.grid, c->stream)
+                            : bitwise::launch_stage(g.lim, a, g.grid, c->stream);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -437,7 +445,8 @@ extern "C" int mbm_create_batch(const mbm_block_desc* blocks, int nblocks, const
   *out = nullptr;
   std::string why;
   if (!blocks || nblocks < 1 || nblocks > 65535) return fail(nullptr, MBM_EINVAL, "need 1..65535 blocks");
-  if (params->mode != MBM_MODE_EXACT) return fail(nullptr, MBM_EINVAL, "unknown arithmetic mode");
+  if (params->mode != MBM_MODE_EXACT && params->mode != MBM_MODE_FAST)
+    return fail(nullptr, MBM_EINVAL, "unknown arithmetic mode");
   // cases tile the block array; sync codes become global block numbers
   std::vector<mbm_block_desc> glob(blocks, blocks + nblocks);
   std::vector<int> blk_case(nblocks, -1);
@@ -579,7 +588,8 @@ extern "C" int mbm_create_batch(const mbm_block_desc* blocks, int nblocks, const
 
   // work table and grid
   CKC(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device));
-  c->ctas_per_sm = stage_ctas_per_sm();
+  c->fast = params->mode == MBM_MODE_FAST;
+  c->ctas_per_sm = c->fast ? fastmath::stage_ctas_per_sm() : bitwise::stage_ctas_per_sm();
   long long max_items = 0;
   for (auto& d : c->hblk) max_items += (long long)((d.nxp - 3 + STRIP - 1) / STRIP) * ((d.nyp - 3 + 7) / 8 + 1);
   CKC(cudaMalloc(&c->dwork, sizeof(Work) * std::max<long long>(1, max_items)));

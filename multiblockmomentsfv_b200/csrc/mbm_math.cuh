@@ -1,4 +1,5 @@
-// mbm_math.cuh -- per-cell and per-face FP64 arithmetic of the Grad-13 Heun stage.
+// mbm_math.cuh -- per-cell and per-face FP64 arithmetic of the Grad-13 Heun stage,
+// in namespace mbm::MBM_ARITH (bitwise by default, fastmath under MBM_FAST_ARITH).
 //
 // Bitwise mode: every expression keeps the operand order and association of the
 // reference expression it restates (file:line cited per function), the file is
@@ -12,7 +13,15 @@
 
 #include "mbm_internal.h"
 
+#ifndef MBM_ARITH
+#define MBM_ARITH bitwise
+#endif
+#ifndef MBM_FAST_ARITH
+#define MBM_FAST_ARITH 0
+#endif
+
 namespace mbm {
+namespace MBM_ARITH {
 
 // the reference's max/min/sgn (src/tools.h:3-17): a > b ? a : b etc.
 __device__ __forceinline__ double rmax(double a, double b) { return a > b ? a : b; }
@@ -34,6 +43,16 @@ __device__ __forceinline__ double rsgn(double a) { return a == 0 ? 0.0 : (a < 0 
 // recomputes its quotients with IEEE division in a cold, outlined path.  Zero
 // numerators take x*r, the signed zero of x/y.  Checked against x/y on the host
 // for 2e8 random operand pairs and by every bitwise parity test.
+//
+// Fast arithmetic (MBM_FAST_ARITH, MBM_MODE_FAST): the quotient is RN(x*r) without
+// the correction, within one unit in the last place of x/y, and no range flag is
+// kept (the cold IEEE paths become dead code); the file is then compiled with
+// multiply-add contraction.
+#if MBM_FAST_ARITH
+__device__ __forceinline__ bool mk_in(double) { return true; }
+
+__device__ __forceinline__ double mk_div(double x, double, double r) { return x * r; }
+#else
 __device__ __forceinline__ bool mk_in(double x) {
   const long long b = __double_as_longlong(x);
   return (((unsigned)(b >> 52) & 0x7ffu) - 543u <= 960u) || ((b << 1) == 0);
@@ -44,6 +63,7 @@ __device__ __forceinline__ double mk_div(double x, double y, double r) {
   const double m = fma(fma(-q, y, x), r, q);
   return ((__double_as_longlong(x) << 1) == 0) ? q : m;
 }
+#endif
 
 __device__ __noinline__ double div_ieee(double x, double y) { return x / y; }
 
@@ -340,4 +360,5 @@ __device__ __forceinline__ double hll(const double (&PL)[NV], const double (&PR)
   return cMax;
 }
 
+}  // namespace MBM_ARITH
 }  // namespace mbm

@@ -30,8 +30,10 @@
 #include "mbm_internal.h"
 
 namespace mbm {
+namespace bitwise {
 cudaError_t launch_stage(int lim, const StageArgs& a, int grid, cudaStream_t s);
 int stage_ctas_per_sm();
+}
 void set_global_error(const std::string& msg);   // read back by mbm_last_error(NULL)
 }  // namespace mbm
 
@@ -162,8 +164,8 @@ extern "C" int mbm_stage_noalloc(const mbm_block_desc* blocks, int nblocks, cons
   a.sel_in = SEL_CUR;
   a.sel_d0 = heun ? SEL_TMP : SEL_CUR;
   a.sel_out = SEL_OTHER;
-  const long long grid = std::min<long long>((nwork + 3) / 4, (long long)sm * stage_ctas_per_sm());
-  e = launch_stage(limiter, a, (int)grid, s);
+  const long long grid = std::min<long long>((nwork + 3) / 4, (long long)sm * bitwise::stage_ctas_per_sm());
+  e = bitwise::launch_stage(limiter, a, (int)grid, s);
   if (!e) e = cudaMemcpyAsync(h_lam, dlam, sizeof(unsigned long long) * 6 * nblocks, cudaMemcpyDeviceToHost, s);
   if (!e) e = cudaStreamSynchronize(s);
   if (e) return fail(MBM_ECUDA, cudaGetErrorString(e));

@@ -1,0 +1,275 @@
+// mbm_stage.cuh -- the Heun stage kernel (Update, src/Main.c:297-396), compiled once per
+// arithmetic mode: mbm_kernels.cu instantiates it in namespace mbm::bitwise (with
+// -fmad=false), mbm_stage_fast.cu in mbm::fastmath (MBM_FAST_ARITH, -fmad=true).
+//
+// One warp owns a strip of 28 output columns plus a 2-column halo on each side
+// (lane l <-> column I0 - 2 + l) and a segment of rows, and marches up the segment.
+// Iteration r loads the moments of row r, forms its projected primitives (raw
+// Primitive on the outermost ring, relaxed otherwise) into a three-row window in
+// shared memory, the y slopes of row r-1 and the y-face flux between rows r-2 and
+// r-1, then the x slopes and x-face states of row r-2 through warp shuffles, its
+// x-face fluxes and its update.  Warps are independent (no barrier); a persistent
+// grid takes work items (block, strip, segment) from an atomic counter.  Every
+// cell's update keeps the reference's accumulation order
+//   New = ((((R + dtdx*F[i-1/2]) + dtdy*G[j-1/2]) - dtdy*G[j+1/2]) - dtdx*F[i+1/2])
+// (its x-outer / y-inner face loop, src/Main.c:353-384), then *0.5 in stage 2.
+// The CFL maxima cover ghost faces and cells exactly as the reference's loops do.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mbm_internal.h"
+#include "mbm_math.cuh"
+
+namespace mbm {
+namespace MBM_ARITH {
+
+// moments of a state at rest with rho = theta = 1: fed to lanes and rows that fall
+// outside the padded grid, whose results are never used
+__device__ __forceinline__ void benign(double (&U)[NV]) {
+  U[0] = 1.0; U[1] = 0.0; U[2] = 0.0; U[3] = 1.5; U[4] = 1.0;
+  U[5] = 0.0; U[6] = 1.0; U[7] = 0.0; U[8] = 0.0;
+}
+
+__device__ __forceinline__ void load_cell(const double* __restrict__ base, long long plane,
+                                          long long idx, double (&U)[NV]) {
+#pragma unroll
+  for (int n = 0; n < NV; n++) U[n] = __ldg(base + n * plane + idx);
+}
+
+// Rolling state of one warp, lane fastest (conflict-free 8-byte accesses): the
+// projected primitives of three consecutive rows, the lower state of the next
+// y face and the y flux of the face below the row being finished.
+struct WarpWindow {
+  double P[3][NV][32];
+  double lo[NV][32];
+  double G[NV][32];
+};
+constexpr int STAGE_WARPS = 4;
+#ifndef STAGE_MIN_CTAS
+#define STAGE_MIN_CTAS 3   // CTAs per SM the register budget is sized for (168 registers)
+#endif
+
+template <int HEUN, int LIM>
+__device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, const int lane,
+                                           WarpWindow& win) {
+  const BlockDev B = a.blk[w.blk];
+  const CaseDev& cs = a.cases[B.case_id];
+  if (cs.done) return;
+  const int cur = cs.cur;
+  const double dt = cs.dt, Fx = cs.F;
+  const Recip Kn(cs.Kn);
+  const double* __restrict__ in = a.buf[phys_layer(a.sel_in, cur)] + B.off;
+  const double* __restrict__ d0 = a.buf[phys_layer(a.sel_d0, cur)] + B.off;
+  double* __restrict__ out = a.buf[phys_layer(a.sel_out, cur)] + B.off;
+  const int nxp = B.nxp, nyp = B.nyp, pitch = B.pitch;
+  const long long plane = B.plane;
+  const int C = w.I0 - 2 + lane;
+  const bool col_in = C >= 0 && C < nxp;
+  const bool col_ring = C == 0 || C == nxp - 1;
+  const bool col_face = C >= 1 && C <= nxp - 3;      // face loop range (src/Main.c:353-354)
+  const bool col_cell = C >= 1 && C <= nxp - 2;      // relaxation range (src/Main.c:320-321)
+  const bool col_out = lane >= 2 && lane <= 29 && C >= NG && C <= nxp - 1 - NG;
+  const bool ylane = lane >= 2 && lane <= 29;        // owners of this strip's y faces
+  const double dtdx = dt / B.dx, dtdy = dt / B.dy;
+  const Recip rdx(B.dx), rdy(B.dy);   // dx, dy in the safe range (checked at creation)
+  const double hdx = 0.5 * B.dx, hdy = 0.5 * B.dy;
+  double lamx = 0.0, lamy = 0.0, prod = 0.0;
+  bool nonfinite = false;
+
+  // The march: iteration r forms the primitives of row r, the y slope of row r-1
+  // and the y face (r-2 | r-1), then finishes row J = r-2 (x face, update).
+  const int rs = w.J0 >= 2 ? w.J0 - 2 : w.J0 - 1;
+  int s0 = rs % 3;                 // window slot of row r
+  for (int r = rs; r <= w.J1 + 1; r++) {
+    const int sm1 = s0 == 0 ? 2 : s0 - 1, sm2 = sm1 == 0 ? 2 : sm1 - 1;
+    // (a) projected primitives of row r: Aux.Prim (src/Main.c:314-336)
+    {
+      double U[NV], Q[NV];
+      const bool ok = col_in && r >= 0 && r < nyp;
+      if (ok) load_cell(in, plane, (long long)r * pitch + C + 1, U);
+      else benign(U);
+      primitive(U, Q);
+      if (ok && col_cell && r >= 1 && r <= nyp - 2) {
+        const double c = relax_cfl<2 * HEUN>(Q, dt, Kn);
+        if (c > prod) prod = c;
+      }
+      if (!(col_ring || r == 0 || r == nyp - 1)) {
+        double V[NV];
+        relax<2 * HEUN + 1>(Q, V, dt, Kn, Fx);
+        primitive(V, Q);
+      }
+#pragma unroll
+      for (int n = 0; n < NV; n++) win.P[s0][n][lane] = Q[n];
+    }
+    // (b) y slope of row r-1 (src/Main.c:348-349) and the y face (r-2 | r-1)
+    double G[NV];
+    const bool face_now = r >= rs + 3;
+    if (r >= rs + 2) {
+      double hi[NV], S[NV];
+      bool sbad = false;
+#pragma unroll
+      for (int n = 0; n < NV; n++) {
+        const double pm = win.P[sm2][n][lane], p0 = win.P[sm1][n][lane], pp = win.P[s0][n][lane];
+        const double L = limit<LIM>(p0 - pm, pp - p0);
+        sbad |= !mk_in(L);
+        S[n] = mk_div(L, rdy.y, rdy.r);
+      }
+      if (__builtin_expect(sbad, 0)) {
+#pragma unroll
+        for (int n = 0; n < NV; n++) {
+          const double pm = win.P[sm2][n][lane], p0 = win.P[sm1][n][lane], pp = win.P[s0][n][lane];
+          S[n] = div_ieee(limit<LIM>(p0 - pm, pp - p0), rdy.y);
+        }
+      }
+#pragma unroll
+      for (int n = 0; n < NV; n++) {
+        const double p0 = win.P[sm1][n][lane];
+        hi[n] = p0 - hdy * S[n];
+        G[n] = p0 + hdy * S[n];               // lower state of the next face, parked in G
+      }
+      if (face_now && ylane) {
+        double lo[NV];
+#pragma unroll
+        for (int n = 0; n < NV; n++) {
+          lo[n] = win.lo[n][lane];
+          win.lo[n][lane] = G[n];
+        }
+        const double lam = hll<2>(lo, hi, G);
+        const int J = r - 2;
+        if (col_face && J >= 1 && J <= nyp - 3 && lam > lamy) lamy = lam;
+      } else {
+#pragma unroll
+        for (int n = 0; n < NV; n++) win.lo[n][lane] = G[n];
+      }
+    }
+    // (c) row J = r-2: x slope, x face C | C+1 (src/Main.c:346-347, 372-378), update
+    const int J = r - 2;
+    if (J >= w.J0 && J < w.J1) {
+      double P0[NV], Sx[NV], lo[NV], hi[NV], F[NV];
+      bool xbad = false;
+#pragma unroll
+      for (int n = 0; n < NV; n++) {
+        P0[n] = win.P[sm2][n][lane];
+        const double pl = __shfl_up_sync(0xffffffffu, P0[n], 1);
+        const double pr = __shfl_down_sync(0xffffffffu, P0[n], 1);
+        const double L = limit<LIM>(P0[n] - pl, pr - P0[n]);
+        xbad |= !mk_in(L);
+        Sx[n] = mk_div(L, rdx.y, rdx.r);
+      }
+      if (__builtin_expect(__any_sync(0xffffffffu, xbad), 0)) {   // warp-uniform cold path
+#pragma unroll
+        for (int n = 0; n < NV; n++) {
+          const double pl = __shfl_up_sync(0xffffffffu, P0[n], 1);
+          const double pr = __shfl_down_sync(0xffffffffu, P0[n], 1);
+          Sx[n] = div_ieee(limit<LIM>(P0[n] - pl, pr - P0[n]), rdx.y);
+        }
+      }
+#pragma unroll
+      for (int n = 0; n < NV; n++) {
+        lo[n] = P0[n] + hdx * Sx[n];
+        hi[n] = __shfl_down_sync(0xffffffffu, P0[n] - hdx * Sx[n], 1);
+      }
+#pragma unroll
+      for (int n = 0; n < NV; n++) F[n] = 0.0;
+      if (lane >= 1 && lane <= 29) {
+        const double lam = hll<1>(lo, hi, F);
+        if (col_face && J >= 1 && J <= nyp - 3 && lam > lamx) lamx = lam;
+      }
+      double Fm[NV];
+#pragma unroll
+      for (int n = 0; n < NV; n++) Fm[n] = __shfl_up_sync(0xffffffffu, F[n], 1);
+      // cell update of row J (src/Main.c:323-331, 367-393)
+      if (col_out && J >= NG && J <= nyp - 1 - NG) {
+        const long long idx = (long long)J * pitch + C + 1;
+        double U[NV], Q[NV], R[NV];
+        load_cell(in, plane, idx, U);
+        primitive(U, Q);
+        relax<2 * HEUN>(Q, R, dt, Kn, Fx);
+        if (HEUN == 1) {
+          double R0[NV];
+          load_cell(d0, plane, idx, U);
+          primitive(U, Q);
+          relax<-1>(Q, R0, dt, Kn, Fx);
+#pragma unroll
+          for (int n = 0; n < NV; n++) R[n] += R0[n];
+        }
+#pragma unroll
+        for (int n = 0; n < NV; n++) {
+          double v = R[n];
+          v += dtdx * Fm[n];
+          v += dtdy * win.G[n][lane];
+          v -= dtdy * G[n];
+          v -= dtdx * F[n];
+          if (HEUN == 1) v = 0.5 * v;
+          out[n * plane + idx] = v;
+          nonfinite |= (__double2hiint(v) & 0x7ff00000) == 0x7ff00000;
+        }
+      }
+    }
+    if (face_now && ylane) {
+#pragma unroll
+      for (int n = 0; n < NV; n++) win.G[n][lane] = G[n];
+    }
+    s0 = s0 == 2 ? 0 : s0 + 1;
+  }
+
+  // per-block maxima; the values are >= 0 (or NaN, which never passes a '>' test
+  // above), so their bit patterns order like the values
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lamx = fmax(lamx, __shfl_xor_sync(0xffffffffu, lamx, o));
+    lamy = fmax(lamy, __shfl_xor_sync(0xffffffffu, lamy, o));
+    prod = fmax(prod, __shfl_xor_sync(0xffffffffu, prod, o));
+  }
+  // failure detection: a NaN or infinity in a written cell marks the case
+  if (__any_sync(0xffffffffu, nonfinite) && lane == 0) atomicOr(&a.cases[B.case_id].nonfinite, 1);
+  if (lane == 0) {
+    unsigned long long* slot = a.lam + ((size_t)w.blk * 2 + HEUN) * 3;
+    if (lamx > 0.0) atomicMax(slot + 0, (unsigned long long)__double_as_longlong(lamx));
+    if (lamy > 0.0) atomicMax(slot + 1, (unsigned long long)__double_as_longlong(lamy));
+    if (prod > 0.0) atomicMax(slot + 2, (unsigned long long)__double_as_longlong(prod));
+  }
+}
+
+// Persistent grid (as many CTAs as fit on the SMs); every warp takes the next work
+// item from a counter until the table is exhausted, so uneven blocks and the last
+// wave balance themselves.
+template <int HEUN, int LIM>
+__global__ void __launch_bounds__(32 * STAGE_WARPS, STAGE_MIN_CTAS) stage_kernel(const StageArgs a) {
+  __shared__ WarpWindow win[STAGE_WARPS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    int w = 0;
+    if (lane == 0) w = atomicAdd(a.queue, 1);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (w >= a.nwork) break;
+    stage_item<HEUN, LIM>(a, a.work[w], lane, win[warp]);
+  }
+}
+
+int stage_ctas_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<1, 4>, 32 * STAGE_WARPS, 0);
+  return n > 0 ? n : 1;
+}
+
+template <int HEUN>
+static cudaError_t launch_stage_lim(int lim, const StageArgs& a, int grid, cudaStream_t s) {
+  switch (lim) {
+    case 0: stage_kernel<HEUN, 0><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
+    case 1: stage_kernel<HEUN, 1><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
+    case 2: stage_kernel<HEUN, 2><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
+    case 3: stage_kernel<HEUN, 3><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
+    default: stage_kernel<HEUN, 4><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage(int lim, const StageArgs& a, int grid, cudaStream_t s) {
+  return a.heun ? launch_stage_lim<1>(lim, a, grid, s) : launch_stage_lim<0>(lim, a, grid, s);
+}
+
+}  // namespace MBM_ARITH
+}  // namespace mbm

@@ -20,6 +20,7 @@
  */
 #include <stdio.h>
 #include <stdlib.h>
+#include <string.h>
 #include <sys/time.h>
 
 #include "database_range.h"
@@ -65,7 +66,8 @@ static void create(DB_Block *B, int bMax)
   p.Kn = Kn;
   p.F = F;
   p.limiter = Limiter;
-  p.mode = MBM_MODE_EXACT;
+  /* MBM_MODE=fast selects the fast-arithmetic stage kernel (not bitwise) */
+  p.mode = (getenv("MBM_MODE") && !strcmp(getenv("MBM_MODE"), "fast")) ? MBM_MODE_FAST : MBM_MODE_EXACT;
   p.device = getenv("MBM_DEVICE") ? atoi(getenv("MBM_DEVICE")) : 0;
   p.show_every = 20;
   p.max_attempts = 0;

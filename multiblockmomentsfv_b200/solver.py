@@ -31,13 +31,14 @@ class Solver:
 
     def __init__(self, deck: bf.Deck, scenario: Optional[sc.Scenario] = None, device: int = 0,
                  show_every: int = 20, stream: Optional[int] = None, segment_rows: int = 0,
-                 max_attempts: int = 0, adjoint: bool = False):
+                 max_attempts: int = 0, adjoint: bool = False, mode: str = "exact"):
+        """mode: "exact" (bit for bit the reference) or "fast" (MBM_MODE_FAST)."""
         self.deck = deck
         self.scenario = scenario
         self.L = _abi.lib()
         self._descs = _abi.block_descs(deck.blocks)
         p = _abi.Params()
-        p.Kn, p.F, p.limiter, p.mode = deck.Kn, deck.F, deck.limiter, _abi.MODE_EXACT
+        p.Kn, p.F, p.limiter, p.mode = deck.Kn, deck.F, deck.limiter, _abi.MODES[mode]
         p.device, p.show_every, p.max_attempts, p.segment_rows = device, show_every, max_attempts, segment_rows
         p.stream = stream
         p.adjoint = 1 if adjoint else 0
@@ -170,8 +171,8 @@ class BatchSolver:
     one device context, advanced together by one CUDA-graph loop with per-case dt."""
 
     def __init__(self, cases, device: int = 0, show_every: int = 0, stream: Optional[int] = None,
-                 segment_rows: int = 0, max_attempts: int = 0):
-        """cases: list of (Deck, Scenario or None)."""
+                 segment_rows: int = 0, max_attempts: int = 0, mode: str = "exact"):
+        """cases: list of (Deck, Scenario or None); mode "exact" or "fast"."""
         self.cases = list(cases)
         self.L = _abi.lib()
         blocks, descs = [], (_abi.CaseDesc * len(self.cases))()
@@ -186,7 +187,7 @@ class BatchSolver:
         self._bd = _abi.block_descs(blocks)
         self._cd = descs
         p = _abi.Params()
-        p.mode, p.device, p.show_every, p.max_attempts, p.segment_rows = (_abi.MODE_EXACT, device,
+        p.mode, p.device, p.show_every, p.max_attempts, p.segment_rows = (_abi.MODES[mode], device,
                                                                           show_every, max_attempts, segment_rows)
         p.stream = stream
         p.Kn, p.limiter = self.cases[0][0].Kn, self.cases[0][0].limiter
@@ -314,11 +315,11 @@ def ghost_map(blocks: Sequence[bf.Block]) -> np.ndarray:
 
 
 def run(deck: bf.Deck, scenario: sc.Scenario, out_dir: str, single: bool = True, device: int = 0,
-        verbose: bool = True, show_every: int = 20):
+        verbose: bool = True, show_every: int = 20, mode: str = "exact"):
     """The reference's main() loop on the device: initial state and output at t=0,
     then Steps + Output per output time (src/Main.c:138-156).  Returns (writer, steps)."""
     w = out.Writer(out_dir, deck, scenario.type_name, single)
-    with Solver(deck, scenario, device=device, show_every=show_every) as s:
+    with Solver(deck, scenario, device=device, show_every=show_every, mode=mode) as s:
         s.initialise()
         w.write_solver(s, 0.0, -1)
         t, nmax = 0.0, 0

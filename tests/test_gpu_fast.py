@@ -1,0 +1,137 @@
+"""MBM_MODE_FAST (multiply-add contraction, reciprocal-multiply quotients) against the
+bitwise mode, which equals the reference bit for bit (test_gpu_parity, test_gpu_dropin):
+per output field, max |fast - reference| / max |reference| over the interior stays at or
+below 1e-10 after one step and 1e-8 at the end time, and the reference's regression gate
+(|a - b| <= 1e-10 + 1e-8 |b| at every point, tools/compare_solution.py's Float64 defaults)
+passes."""
+import numpy as np
+import pytest
+
+import helpers as H
+from multiblockmomentsfv_b200 import blockfile as bf
+from multiblockmomentsfv_b200 import output
+from multiblockmomentsfv_b200 import scenario as sc
+from multiblockmomentsfv_b200 import solver as sv
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = "rho vx vy T p Pxx Pxy Pyy qx qy".split()
+
+
+def _fields(layers):
+    return [output.physical_fields(U[bf.NG:-bf.NG, bf.NG:-bf.NG]) for U in layers]
+
+
+def _field_errors(fast, ref):
+    """max over blocks and cells of |a - b| per field, over max |b| per field."""
+    a, b = _fields(fast), _fields(ref)
+    num = np.max([np.abs(x - y).reshape(-1, 10).max(axis=0) for x, y in zip(a, b)], axis=0)
+    den = np.max([np.abs(y).reshape(-1, 10).max(axis=0) for y in b], axis=0)
+    return dict(zip(FIELDS, num / den))
+
+
+def _run(deck, scn, mode, tend, max_steps=0):
+    with sv.Solver(deck, scn, mode=mode, show_every=0) as s:
+        s.initialise()
+        t, n, r = s.steps(0.0, tend, max_steps=max_steps)
+        return s.layers(sv.L_DATA), t, n, r
+
+
+def test_fast_one_step_full_size():
+    d = H.quadrant_deck(1024, Kn=0.01)
+    scn = sc.Scenario.seeded_quadrant(2024)
+    ref, _, n0, _ = _run(d, scn, "exact", 1.0, max_steps=1)
+    fast, _, n1, _ = _run(d, scn, "fast", 1.0, max_steps=1)
+    assert n0 == n1 == 1
+    err = _field_errors(fast, ref)
+    print("fast vs exact after one step: " + ", ".join("%s %.1e" % kv for kv in err.items()))
+    assert max(err.values()) <= 1e-10, err
+    assert max(err.values()) > 0.0          # the modes do differ: this is not the bitwise kernel
+
+
+@pytest.mark.parametrize("limiter", [bf.LIM_NONE, bf.LIM_SUPERBEE, bf.LIM_HARMONIC])
+def test_fast_end_time_limiters(limiter):
+    d = H.quadrant_deck(96, Kn=0.005, limiter=limiter)
+    scn = sc.Scenario.seeded_quadrant(7)
+    ref, t0, n0, r0 = _run(d, scn, "exact", 0.3)
+    fast, t1, n1, r1 = _run(d, scn, "fast", 0.3)
+    assert (t0, n0, r0) == (t1, n1, r1)
+    err = _field_errors(fast, ref)
+    assert max(err.values()) <= 1e-8, err
+
+
+def _run_perturbed(deck, scn, tend, rel=1e-15, seed=0):
+    """Bitwise mode (= the reference) from the initial state times (1 + rel * N(0, 1))."""
+    rng = np.random.default_rng(seed)
+    with sv.Solver(deck, scn, mode="exact", show_every=0) as s:
+        s.initialise()
+        for b in range(len(deck.blocks)):
+            U = s.download(sv.L_DATA, b)
+            s.upload(sv.L_DATA, b, U * (1 + rel * rng.standard_normal(U.shape)))
+        s.set_boundary(sv.L_DATA, 0.0)
+        t, n, r = s.steps(0.0, tend)
+        return s.layers(sv.L_DATA), t, n, r
+
+
+def test_fast_minmod_within_the_references_own_spread():
+    """Minmod on the quadrant state amplifies round-off exponentially in the reference
+    itself: its results from initial states 1e-15 apart differ by ~1e-3 at t = 0.3.
+    Up to t = 0.1 the 1e-8 bound holds; at t = 0.3 the fast mode stays within the
+    spread the reference shows under a 1e-15 perturbation of its input."""
+    d = H.quadrant_deck(96, Kn=0.005, limiter=bf.LIM_MINMOD)
+    scn = sc.Scenario.seeded_quadrant(7)
+    ref, t0, n0, r0 = _run(d, scn, "exact", 0.1)
+    fast, t1, n1, r1 = _run(d, scn, "fast", 0.1)
+    assert (t0, n0, r0) == (t1, n1, r1)
+    assert max(_field_errors(fast, ref).values()) <= 1e-8
+    ref, _, n0, _ = _run(d, scn, "exact", 0.3)
+    fast, _, n1, _ = _run(d, scn, "fast", 0.3)
+    pert, _, n2, _ = _run_perturbed(d, scn, 0.3)
+    assert n0 == n1 == n2
+    e_fast = max(_field_errors(fast, ref).values())
+    e_ref = max(_field_errors(pert, ref).values())
+    print("minmod, t = 0.3: fast vs exact %.1e, exact vs exact from a 1e-15-perturbed state %.1e" % (e_fast, e_ref))
+    assert e_ref > 1e-8                       # the case is ill-conditioned in the reference itself
+    assert e_fast <= 100 * e_ref
+
+
+def test_fast_end_time_benchmark():
+    """The 4 x 1024^2 workload to t = 0.3: per-field error and the pointwise gate."""
+    d = H.quadrant_deck(1024, Kn=0.01)
+    scn = sc.Scenario.seeded_quadrant(2024)
+    ref, t0, n0, r0 = _run(d, scn, "exact", 0.3)
+    fast, t1, n1, r1 = _run(d, scn, "fast", 0.3)
+    assert (t0, n0, r0) == (t1, n1, r1)
+    err = _field_errors(fast, ref)
+    print("fast vs exact at t = 0.3 (4 x 1024^2, %d steps): %s" %
+          (n0, ", ".join("%s %.1e" % kv for kv in err.items())))
+    assert max(err.values()) <= 1e-8, err
+    for a, b in zip(_fields(fast), _fields(ref)):
+        assert np.all(np.abs(a - b) <= 1e-10 + 1e-8 * np.abs(b))
+
+
+def test_fast_reference_deck_regression_gate(tmp_path):
+    """cases/squareSmall.txt (Riemann2D, 7 output levels to t = 0.3) written with
+    -double in both modes; the reference's regression comparison at its Float64
+    defaults passes."""
+    d = H.deck("squareSmall")
+    scn = sc.Scenario.named("riemann2d")
+    w_ref, n_ref = sv.run(d, scn, str(tmp_path / "exact"), single=False, verbose=False, mode="exact")
+    w_fast, n_fast = sv.run(d, scn, str(tmp_path / "fast"), single=False, verbose=False, mode="fast")
+    assert n_ref == n_fast
+    ok, mx, msg = output.compare(w_fast.base, w_ref.base)
+    assert ok, msg
+
+
+def test_fast_batch_equals_fast_alone():
+    cases = [(H.quadrant_deck(40 + 8 * k, Kn=0.01 * (k + 1), limiter=k % 5), sc.Scenario.seeded_quadrant(k))
+             for k in range(5)]
+    with sv.BatchSolver(cases, mode="fast") as bs:
+        bs.initialise()
+        tb, nb, rb = bs.steps(0.0, 0.05)
+        got = [[bs.download(sv.L_DATA, k, b) for b in range(4)] for k in range(len(cases))]
+    for k, (d, scn) in enumerate(cases):
+        layers, t, n, r = _run(d, scn, "fast", 0.05)
+        assert (t, n, r) == (tb[k], nb[k], rb[k])
+        for b in range(4):
+            H.assert_bitwise(got[k][b], layers[b], f"case {k} block {b + 1}")
