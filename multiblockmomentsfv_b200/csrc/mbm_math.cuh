@@ -19,6 +19,10 @@
 #ifndef MBM_FAST_ARITH
 #define MBM_FAST_ARITH 0
 #endif
+#if MBM_FAST_ARITH
+#define MBM_HD __host__ __device__ __forceinline__
+#include "mbm_adjoint_math.cuh"   // primitive-form Conservative and Grad-13 flux
+#endif
 
 namespace mbm {
 namespace MBM_ARITH {
@@ -66,6 +70,13 @@ __device__ __forceinline__ double mk_div(double x, double y, double r) {
 #endif
 
 __device__ __noinline__ double div_ieee(double x, double y) { return x / y; }
+
+// a quotient with its own denominator: IEEE division (bitwise), x * RN(1/y) (fast)
+#if MBM_FAST_ARITH
+__device__ __forceinline__ double fdiv(double x, double y) { return x * __drcp_rn(y); }
+#else
+__device__ __forceinline__ double fdiv(double x, double y) { return x / y; }
+#endif
 
 struct Recip {        // 1/y for a denominator shared by several quotients
   double y, r;
@@ -255,10 +266,10 @@ __device__ __forceinline__ void flux_normal(const double (&U)[NV], double (&F)[N
 // damping factor of the direct production integration (src/Flux.c:213-223)
 template <int FLAG>
 __device__ __forceinline__ double rdamp(double z) {
-  if (FLAG == -1 || FLAG == 0) return (1 + 0.5 * z - 0.25 * z * z) / (1 + z + 0.25 * z * z);
-  if (FLAG == 1) return (1 + z) / (1 + z + 0.25 * z * z);
-  if (FLAG == 2) return (1 + 0.5 * z) / (1 + 0.5 * z);
-  return 1.0 / (1 + 0.5 * z);
+  if (FLAG == -1 || FLAG == 0) return fdiv(1 + 0.5 * z - 0.25 * z * z, 1 + z + 0.25 * z * z);
+  if (FLAG == 1) return fdiv(1 + z, 1 + z + 0.25 * z * z);
+  if (FLAG == 2) return fdiv(1 + 0.5 * z, 1 + 0.5 * z);
+  return fdiv(1.0, 1 + 0.5 * z);
 }
 
 // ProductionsDirect (src/Flux.c:230-267) with CollFreq and ExternalForce
@@ -315,12 +326,58 @@ __device__ __forceinline__ double limit(double d1, double d2) {
   if (LIM == 0) return 0.0;
   if (LIM == 1) return 0.5 * (d1 + d2);
   if (LIM == 2) return 0.5 * (rsgn(d1) + rsgn(d2)) * rmin(fabs(d1), fabs(d2));
-  if (LIM == 3) return d1 * superbee_phi(d2 / d1);
+  if (LIM == 3) return d1 * superbee_phi(fdiv(d2, d1));
   const double eps = 1.0e-10;
   const double w1 = fabs(d1) + eps, w2 = fabs(d2) + eps;
-  return (w1 * d2 + w2 * d1) / (w1 + w2);
+  return fdiv(w1 * d2 + w2 * d1, w1 + w2);
 }
 
+#if MBM_FAST_ARITH
+// FnumHLLE (src/Flux.c:308-379) in primitive form (fast arithmetic): the Grad-13
+// flux straight from the face states -- no Conservative -> Primitive round trip and
+// no rotations (a y face swaps the x and y components, which is what the rotation
+// to the normal (0,1) amounts to); one reciprocal of alpha.  Mathematically the
+// bitwise version below; the rounding differs.
+template <int DIR>
+__device__ __forceinline__ double hll(const double (&PL_)[NV], const double (&PR_)[NV],
+                                      double (&flx)[NV]) {
+  double PL[NV], PR[NV], UL[NV], UR[NV], fL[NV], fR[NV];
+  if (DIR == 2) {
+    mbm_adj::swap_xy(PL_, PL);
+    mbm_adj::swap_xy(PR_, PR);
+  } else {
+#pragma unroll
+    for (int n = 0; n < NV; n++) { PL[n] = PL_[n]; PR[n] = PR_[n]; }
+  }
+  const double cR = 2.0 * sqrt(5.0 / 3 * PR[3]);
+  const double cL = 2.0 * sqrt(5.0 / 3 * PL[3]);
+  mbm_adj::cons(PL, UL);
+  mbm_adj::cons(PR, UR);
+  mbm_adj::gflux_x(PL, fL);
+  mbm_adj::gflux_x(PR, fR);
+  const double vR = PR[1], vL = PL[1];
+  const double cMax = fabs(0.5 * (vL + vR)) + rmax(cR, cL);
+  const double lamL = rmin(vL - cL, 0.0);
+  const double lamR = rmax(vR + cR, 0.0);
+  const double alph = lamR - lamL;
+  double f[NV];
+  if (alph > 0.0) {
+    const double ra = __drcp_rn(alph);
+#pragma unroll
+    for (int n = 0; n < NV; n++) f[n] = (lamR * fL[n] - lamL * fR[n] + lamL * lamR * (UR[n] - UL[n])) * ra;
+  } else {
+#pragma unroll
+    for (int n = 0; n < NV; n++) f[n] = 0.5 * (fL[n] + fR[n]);
+  }
+  if (DIR == 2) {
+    mbm_adj::swap_xy(f, flx);
+  } else {
+#pragma unroll
+    for (int n = 0; n < NV; n++) flx[n] = f[n];
+  }
+  return cMax;
+}
+#else
 // FnumHLLE (src/Flux.c:308-379) for a face with left/right primitives.
 // DIR = 1: x face (normal (1,0)), DIR = 2: y face (normal (0,1)).  The
 // diffusive scale FFlux/GFlux return is 0, so lamDiff(0/(cMax*dx)) is 1 for
@@ -359,6 +416,7 @@ __device__ __forceinline__ double hll(const double (&PL)[NV], const double (&PR)
   }
   return cMax;
 }
+#endif
 
 }  // namespace MBM_ARITH
 }  // namespace mbm
