@@ -303,6 +303,29 @@ __device__ __forceinline__ double relax(const double (&P)[NV], double (&Out)[NV]
   return 0.5 * (1 - d2);
 }
 
+#if MBM_FAST_ARITH
+// Primitive(relax<FLAG>(P)) in primitive form (fast arithmetic): rho and theta kept,
+// the velocity pushed by dt F for flags 0 and 2, T_ij - theta delta_ij scaled by
+// R(z), q by R(2z/3) -- without forming the moments and dividing by rho again
+template <int FLAG>
+__device__ __forceinline__ void relax_prim(const double (&P)[NV], double (&Q)[NV], double dt,
+                                           const Recip& Kn, double F) {
+  const double rho = P[0], th = P[3];
+  const double coll = rho * sqrt(th) * Kn.r * dt;
+  const double d1 = rdamp<FLAG>(coll);
+  const double d2 = rdamp<FLAG>(2.0 / 3 * coll);
+  Q[0] = rho;
+  Q[1] = P[1] + ((FLAG == 0 || FLAG == 2) ? dt * F : 0.0);
+  Q[2] = P[2];
+  Q[3] = th;
+  Q[4] = d1 * (P[4] - th) + th;
+  Q[5] = d1 * P[5];
+  Q[6] = d1 * (P[6] - th) + th;
+  Q[7] = d2 * P[7];
+  Q[8] = d2 * P[8];
+}
+#endif
+
 // only the CFL share of relax<FLAG> (same z, same factor)
 template <int FLAG>
 __device__ __forceinline__ double relax_cfl(const double (&P)[NV], double dt, const Recip& Kn) {

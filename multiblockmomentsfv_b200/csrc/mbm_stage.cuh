@@ -96,9 +96,16 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         if (c > prod) prod = c;
       }
       if (!(col_ring || r == 0 || r == nyp - 1)) {
+#if MBM_FAST_ARITH
+        double V[NV];
+        relax_prim<2 * HEUN + 1>(Q, V, dt, Kn, Fx);
+#pragma unroll
+        for (int n = 0; n < NV; n++) Q[n] = V[n];
+#else
         double V[NV];
         relax<2 * HEUN + 1>(Q, V, dt, Kn, Fx);
         primitive(V, Q);
+#endif
       }
 #pragma unroll
       for (int n = 0; n < NV; n++) win.P[s0][n][lane] = Q[n];
