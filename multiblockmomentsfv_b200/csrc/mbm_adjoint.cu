@@ -79,7 +79,7 @@ __device__ __forceinline__ double slope_at(const AdjArgs& a, const BlockDev& B, 
   const long long i = cidx(B, I, J) + m * B.plane;
   const long long s = dir == 1 ? 1 : B.pitch;
   const double d1 = a.P[i] - a.P[i - s], d2 = a.P[i + s] - a.P[i];
-  return mbm_adj::limit_val(a.limiter, d1, d2) / h;
+  return mbm_adj::limit_val(a.limiter, d1, d2) * mbm_adj::rcp(h);
 }
 
 // pass B: faces (I,J)|(I+1,J) (dir 1) or (I,J)|(I,J+1) (dir 2) next to an output cell
@@ -102,14 +102,14 @@ __global__ void __launch_bounds__(128, 4) adj_faces(AdjArgs a, long long ncell, 
     }
     return;
   }
-  const double h = dir == 1 ? B.dx : B.dy;
+  const double h = dir == 1 ? B.dx : B.dy, rh = mbm_adj::rcp(h);
   const double s = a.heun ? 0.5 : 1.0;
   double PL[NV], PR[NV], fb[NV], gl[NV] = {0}, gr[NV] = {0};
   bool any = false;
   for (int m = 0; m < NV; m++) {
     const double lo = inL ? a.lout[cidx(B, I, J) + m * B.plane] : 0.0;
     const double hi = inR ? a.lout[cidx(B, I2, J2) + m * B.plane] : 0.0;
-    fb[m] = s * a.dt / h * (hi - lo);
+    fb[m] = s * a.dt * rh * (hi - lo);
     any = any || fb[m] != 0.0;
     PL[m] = a.P[cidx(B, I, J) + m * B.plane] + 0.5 * h * slope_at(a, B, I, J, dir, m, h);
     PR[m] = a.P[cidx(B, I2, J2) + m * B.plane] - 0.5 * h * slope_at(a, B, I2, J2, dir, m, h);
@@ -132,7 +132,7 @@ __device__ __forceinline__ void gather_dir(const AdjArgs& a, const BlockDev& B, 
                                            const double* FL, const double* FR, double* Pb) {
   const long long s = dir == 1 ? 1 : B.pitch;
   const int n = dir == 1 ? B.nxp : B.nyp, c = dir == 1 ? I : J;
-  const double h = dir == 1 ? B.dx : B.dy;
+  const double h = dir == 1 ? B.dx : B.dy, rh = mbm_adj::rcp(h);
   const long long i0 = cidx(B, I, J);
   const bool lft = c >= 2, rgt = c <= n - 3;      // slopes of c-1 and c+1 exist (off the ring)
 #pragma unroll 1
@@ -150,19 +150,19 @@ __device__ __forceinline__ void gather_dir(const AdjArgs& a, const BlockDev& B, 
     if (l0 != 0.0) {
       double g1, g2;
       mbm_adj::limit_grad(a.limiter, p0 - pm, pp - p0, &g1, &g2);
-      g += l0 * (g1 - g2) / h;
+      g += l0 * (g1 - g2) * rh;
     }
     const double lm = lft ? 0.5 * h * (flm - frm2) : 0.0;
     if (lm != 0.0) {
       double g1, g2;
       mbm_adj::limit_grad(a.limiter, pm - pm2, p0 - pm, &g1, &g2);
-      g += lm * g2 / h;
+      g += lm * g2 * rh;
     }
     const double lp = rgt ? 0.5 * h * (flp - fr0) : 0.0;
     if (lp != 0.0) {
       double g1, g2;
       mbm_adj::limit_grad(a.limiter, pp - p0, pp2 - pp, &g1, &g2);
-      g -= lp * g1 / h;
+      g -= lp * g1 * rh;
     }
     Pb[m] += g;
   }

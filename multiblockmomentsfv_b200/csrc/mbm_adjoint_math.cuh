@@ -33,6 +33,16 @@ namespace mbm_adj {
 
 constexpr int NV = 9;
 
+// 1/x: the correctly rounded reciprocal on the device, one multiply per quotient
+// after it (the derivatives need no bit-exact quotients)
+MBM_HD double rcp(double x) {
+#ifdef __CUDA_ARCH__
+  return __drcp_rn(x);
+#else
+  return 1.0 / x;
+#endif
+}
+
 // ---------------------------------------------------------------- Conservative
 MBM_HD void cons(const double* P, double* U) {
   const double r = P[0], u = P[1], v = P[2], th = P[3];
@@ -76,16 +86,16 @@ MBM_HD void cons_adj(const double* P, const double* Ub, double* Pb) {
 
 // ------------------------------------------------------------------ Primitive
 MBM_HD void prim(const double* U, double* P) {
-  const double r = U[0];
-  const double u = U[1] / r, v = U[2] / r;
+  const double r = U[0], ir = rcp(r);
+  const double u = U[1] * ir, v = U[2] * ir;
   const double vs = u * u + v * v;
   P[0] = r;
   P[1] = u;
   P[2] = v;
-  P[3] = (2 * U[3] / r - vs) / 3;
-  P[4] = U[4] / r - u * u;
-  P[5] = U[5] / r - u * v;
-  P[6] = U[6] / r - v * v;
+  P[3] = (2 * U[3] * ir - vs) * (1.0 / 3);
+  P[4] = U[4] * ir - u * u;
+  P[5] = U[5] * ir - u * v;
+  P[6] = U[6] * ir - v * v;
   P[7] = U[7] - U[3] * u - r * (P[4] * u + P[5] * v);
   P[8] = U[8] - U[3] * v - r * (P[5] * u + P[6] * v);
 }
@@ -95,6 +105,7 @@ MBM_HD void prim_adj(const double* U, const double* Pb_in, double* Ub) {
   double P[NV];
   prim(U, P);
   const double r = U[0], u = P[1], v = P[2], E = U[3];
+  const double ir = rcp(r), ir2 = ir * ir;
   const double T11 = P[4], T12 = P[5], T22 = P[6];
   double Pb[NV];
   for (int n = 0; n < NV; n++) Pb[n] = Pb_in[n];
@@ -119,26 +130,26 @@ MBM_HD void prim_adj(const double* U, const double* Pb_in, double* Ub) {
   T12b += Pb[5];
   T22b += Pb[6];
   // T22 = U6/r - v^2 ; T12 = U5/r - u v ; T11 = U4/r - u^2
-  U6b += T22b / r;
-  rb += -T22b * U[6] / (r * r);
+  U6b += T22b * ir;
+  rb += -T22b * U[6] * ir2;
   vb += -T22b * 2 * v;
-  U5b += T12b / r;
-  rb += -T12b * U[5] / (r * r);
+  U5b += T12b * ir;
+  rb += -T12b * U[5] * ir2;
   ub += -T12b * v;
   vb += -T12b * u;
-  U4b += T11b / r;
-  rb += -T11b * U[4] / (r * r);
+  U4b += T11b * ir;
+  rb += -T11b * U[4] * ir2;
   ub += -T11b * 2 * u;
   // th = (2 U3/r - u^2 - v^2)/3
   const double thb = Pb[3];
-  U3b += thb * 2 / (3 * r);
-  rb += -thb * 2 * U[3] / (3 * r * r);
-  ub += -thb * 2 * u / 3;
-  vb += -thb * 2 * v / 3;
+  U3b += thb * (2.0 / 3) * ir;
+  rb += -thb * (2.0 / 3) * U[3] * ir2;
+  ub += -thb * (2.0 / 3) * u;
+  vb += -thb * (2.0 / 3) * v;
   // u = U1/r, v = U2/r
-  Ub[1] += ub / r;
-  Ub[2] += vb / r;
-  rb += -(ub * U[1] + vb * U[2]) / (r * r);
+  Ub[1] += ub * ir;
+  Ub[2] += vb * ir;
+  rb += -(ub * U[1] + vb * U[2]) * ir2;
   Ub[0] += rb;
   Ub[3] += U3b;
   Ub[4] += U4b;
@@ -157,14 +168,15 @@ MBM_HD double rdamp(double z, int flag, double* dz) {
     case 2: *dz = 0.0; return 1.0;
     default: N = 1; Nd = 0; D = 1 + 0.5 * z; Dd = 0.5; break;
   }
-  *dz = (Nd * D - N * Dd) / (D * D);
-  return N / D;
+  const double iD = rcp(D);
+  *dz = (Nd * D - N * Dd) * iD * iD;
+  return N * iD;
 }
 
 // relaxation in primitive form: P -> Q (ProductionsDirect's state, src/Flux.c:230-267)
 MBM_HD void relax_p(const double* P, double* Q, double dt, double Kn, double F, int flag) {
   const double r = P[0], th = P[3];
-  const double z = r * sqrt(th) / Kn * dt;
+  const double z = r * sqrt(th) * rcp(Kn) * dt;
   double dd;
   const double d1 = rdamp(z, flag, &dd);
   const double d2 = rdamp(2.0 / 3 * z, flag, &dd);
@@ -183,7 +195,7 @@ MBM_HD void relax_p(const double* P, double* Q, double dt, double Kn, double F, 
 MBM_HD void relax_p_adj(const double* P, const double* Qb, double* Pb, double* Knb, double dt, double Kn,
                         int flag) {
   const double r = P[0], th = P[3];
-  const double z = r * sqrt(th) / Kn * dt;
+  const double z = r * sqrt(th) * rcp(Kn) * dt;
   double r1, r2;
   const double d1 = rdamp(z, flag, &r1);
   const double d2 = rdamp(2.0 / 3 * z, flag, &r2);
@@ -200,9 +212,9 @@ MBM_HD void relax_p_adj(const double* P, const double* Qb, double* Pb, double* K
   const double d2b = Qb[7] * P[7] + Qb[8] * P[8];
   const double zb = d1b * r1 + d2b * (2.0 / 3) * r2;
   if (z != 0.0) {
-    Pb[0] += zb * z / r;
-    Pb[3] += zb * z / (2 * th);
-    *Knb += -zb * z / Kn;
+    Pb[0] += zb * z * rcp(r);
+    Pb[3] += 0.5 * zb * z * rcp(th);
+    *Knb += -zb * z * rcp(Kn);
   }
 }
 
@@ -345,20 +357,21 @@ MBM_HD void hll_p_adj(const double* PL_, const double* PR_, const double* fb_, d
     cons(PR, T);
     for (int n = 0; n < NV; n++) DR += fb[n] * T[n];
     const double D = DR - DL;
-    const double Fd = (lamR * A - lamL * B + lamL * lamR * D) / alph;   // fb . F
-    const double lRb = (A + lamL * D - Fd) / alph;                       // dF/dlamR . fb
-    const double lLb = (-B + lamR * D + Fd) / alph;                      // dF/dlamL . fb
+    const double ia = rcp(alph);
+    const double Fd = (lamR * A - lamL * B + lamL * lamR * D) * ia;     // fb . F
+    const double lRb = (A + lamL * D - Fd) * ia;                         // dF/dlamR . fb
+    const double lLb = (-B + lamR * D + Fd) * ia;                        // dF/dlamL . fb
     // lamL = uL - cL (active), lamR = uR + cR (active); c = 2 sqrt(5 th / 3), dc/dth = (10/3)/c
-    if (aL) { PLb[1] += lLb; PLb[3] += -lLb * (10.0 / 3) / cL; }
-    if (aR) { PRb[1] += lRb; PRb[3] += lRb * (10.0 / 3) / cR; }
-    const double kU = lamL * lamR / alph;
+    if (aL) { PLb[1] += lLb; PLb[3] += -lLb * (10.0 / 3) * rcp(cL); }
+    if (aR) { PRb[1] += lRb; PRb[3] += lRb * (10.0 / 3) * rcp(cR); }
+    const double kU = lamL * lamR * ia;
     for (int n = 0; n < NV; n++) T[n] = -kU * fb[n];
     cons_adj(PL, T, PLb);
-    for (int n = 0; n < NV; n++) T[n] = fb[n] * lamR / alph;
+    for (int n = 0; n < NV; n++) T[n] = fb[n] * lamR * ia;
     gflux_x_adj(PL, T, PLb);
     for (int n = 0; n < NV; n++) T[n] = kU * fb[n];
     cons_adj(PR, T, PRb);
-    for (int n = 0; n < NV; n++) T[n] = -fb[n] * lamL / alph;
+    for (int n = 0; n < NV; n++) T[n] = -fb[n] * lamL * ia;
     gflux_x_adj(PR, T, PRb);
   } else {
     for (int n = 0; n < NV; n++) T[n] = 0.5 * fb[n];
@@ -391,7 +404,7 @@ MBM_HD void limit_grad(int lim, double d1, double d2, double* g1, double* g2) {
     }
     case 3: {
       if (d1 == 0) { *g1 = 0; *g2 = 0; return; }
-      const double th = d2 / d1;
+      const double th = d2 * rcp(d1);
       // L = d1 phi(th):  dL/dd1 = phi - th phi',  dL/dd2 = phi'
       double phi, dphi;
       if (th < 0.0) { phi = 0; dphi = 0; }
@@ -409,8 +422,9 @@ MBM_HD void limit_grad(int lim, double d1, double d2, double* g1, double* g2) {
       const double s1 = d1 < 0 ? -1.0 : 1.0, s2 = d2 < 0 ? -1.0 : 1.0;
       const double N = w1 * d2 + w2 * d1, D = w1 + w2;
       // dN/dd1 = s1 d2 + w2, dN/dd2 = w1 + s2 d1 ; dD/dd1 = s1, dD/dd2 = s2
-      *g1 = ((s1 * d2 + w2) * D - N * s1) / (D * D);
-      *g2 = ((w1 + s2 * d1) * D - N * s2) / (D * D);
+      const double iD2 = rcp(D * D);
+      *g1 = ((s1 * d2 + w2) * D - N * s1) * iD2;
+      *g2 = ((w1 + s2 * d1) * D - N * s2) * iD2;
       return;
     }
   }
@@ -426,7 +440,7 @@ MBM_HD double limit_val(int lim, double d1, double d2) {
       return 0.5 * (s1 + s2) * (fabs(d1) < fabs(d2) ? fabs(d1) : fabs(d2));
     }
     case 3: {
-      const double th = d2 / d1;
+      const double th = d2 * rcp(d1);
       double phi;
       if (th < 0.0) phi = 0;
       else if (th < 0.5) phi = 2 * th;
@@ -438,7 +452,7 @@ MBM_HD double limit_val(int lim, double d1, double d2) {
     default: {
       const double eps = 1.0e-10;
       const double w1 = fabs(d1) + eps, w2 = fabs(d2) + eps;
-      return (w1 * d2 + w2 * d1) / (w1 + w2);
+      return (w1 * d2 + w2 * d1) * rcp(w1 + w2);
     }
   }
 }
