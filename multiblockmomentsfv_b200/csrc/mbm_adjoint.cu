@@ -28,16 +28,24 @@ __device__ __forceinline__ long long cidx(const BlockDev& B, int I, int J) {
   return B.off + (long long)J * B.pitch + I + 1;
 }
 
-// which block and cell a flat thread index covers (blocks in order)
+// Thread mapping: every 128-thread CTA covers a tile of 32 x 4 cells of one block
+// (x fastest), so the y neighbours a cell reads were mostly loaded by the same CTA.
+// Tiles are numbered block by block; k is the flat thread index.
+constexpr int TILE_X = 32, TILE_Y = 4, TILE_T = TILE_X * TILE_Y;
+
 __device__ __forceinline__ bool locate(const BlockDev* blk, int nblk, long long k, int& b, int& I, int& J) {
+  long long tile = k / TILE_T;
+  const int t = (int)(k - tile * TILE_T);
   for (b = 0; b < nblk; b++) {
-    const long long n = (long long)blk[b].nxp * blk[b].nyp;
-    if (k < n) {
-      J = (int)(k / blk[b].nxp);
-      I = (int)(k - (long long)J * blk[b].nxp);
-      return true;
+    const int tx = (blk[b].nxp + TILE_X - 1) / TILE_X, ty = (blk[b].nyp + TILE_Y - 1) / TILE_Y;
+    const long long n = (long long)tx * ty;
+    if (tile < n) {
+      const int jt = (int)(tile / tx), it = (int)(tile - (long long)jt * tx);
+      I = it * TILE_X + (t % TILE_X);
+      J = jt * TILE_Y + (t / TILE_X);
+      return I < blk[b].nxp && J < blk[b].nyp;
     }
-    k -= n;
+    tile -= n;
   }
   return false;
 }
@@ -49,10 +57,10 @@ __device__ __forceinline__ void load9(const double* base, const BlockDev& B, int
 }
 
 // pass A: the forward stage's projected primitives (Aux.Prim, src/Main.c:314-336)
-__global__ void adj_prims(AdjArgs a, long long ncell) {
+__global__ void adj_prims(AdjArgs a, long long nthr) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, J;
-  if (k >= ncell || !locate(a.blk, a.nblk, k, b, I, J)) return;
+  if (k >= nthr || !locate(a.blk, a.nblk, k, b, I, J)) return;
   const BlockDev B = a.blk[b];
   double U[NV], P[NV];
   load9(a.x, B, I, J, U);
@@ -85,11 +93,8 @@ __device__ __forceinline__ double slope_at(const AdjArgs& a, const BlockDev& B, 
 // pass B: faces (I,J)|(I+1,J) (dir 1) or (I,J)|(I,J+1) (dir 2) next to an output cell
 // 128 registers: four 128-thread CTAs per SM hide the neighbour loads better than
 // the spill-free allocation at half the occupancy
-__global__ void __launch_bounds__(128, 4) adj_faces(AdjArgs a, long long ncell, int dir) {
-  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b, I, J;
-  if (k >= ncell || !locate(a.blk, a.nblk, k, b, I, J)) return;
-  const BlockDev B = a.blk[b];
+__device__ __forceinline__ void face_adj(const AdjArgs& a, const BlockDev& B, int I, int J, int dir,
+                                         double* __restrict__ FL, double* __restrict__ FR) {
   const int I2 = dir == 1 ? I + 1 : I, J2 = dir == 1 ? J : J + 1;
   const bool face = I2 < B.nxp && J2 < B.nyp;
   const bool inL = inner(B, I, J), inR = face && inner(B, I2, J2);
@@ -97,8 +102,8 @@ __global__ void __launch_bounds__(128, 4) adj_faces(AdjArgs a, long long ncell, 
     const long long i = cidx(B, I, J);
 #pragma unroll
     for (int m = 0; m < NV; m++) {
-      a.FL[i + m * B.plane] = 0.0;
-      a.FR[i + m * B.plane] = 0.0;
+      FL[i + m * B.plane] = 0.0;
+      FR[i + m * B.plane] = 0.0;
     }
     return;
   }
@@ -118,9 +123,20 @@ __global__ void __launch_bounds__(128, 4) adj_faces(AdjArgs a, long long ncell, 
   const long long i = cidx(B, I, J);
 #pragma unroll
   for (int m = 0; m < NV; m++) {
-    a.FL[i + m * B.plane] = gl[m];
-    a.FR[i + m * B.plane] = gr[m];
+    FL[i + m * B.plane] = gl[m];
+    FR[i + m * B.plane] = gr[m];
   }
+}
+
+// both faces of a cell that lie on its high side: (I,J)|(I+1,J) and (I,J)|(I,J+1)
+__global__ void __launch_bounds__(128, 4) adj_faces(AdjArgs a, long long nthr, double* FLx, double* FRx,
+                                                    double* FLy, double* FRy) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b, I, J;
+  if (k >= nthr || !locate(a.blk, a.nblk, k, b, I, J)) return;
+  const BlockDev B = a.blk[b];
+  face_adj(a, B, I, J, 1, FLx, FRx);
+  face_adj(a, B, I, J, 2, FLy, FRy);
 }
 
 // adjoint of the reconstruction and slopes along one direction, accumulated into Pb;
@@ -169,12 +185,9 @@ __device__ __forceinline__ void gather_dir(const AdjArgs& a, const BlockDev& B, 
 }
 
 // pass C: per cell, back to the stage input (and Data0)
-__global__ void __launch_bounds__(128, 4) adj_cells(AdjArgs a, long long ncell, const double* FLx,
-                                                    const double* FRx, const double* FLy, const double* FRy) {
-  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int b, I, J;
-  if (k >= ncell || !locate(a.blk, a.nblk, k, b, I, J)) return;
-  const BlockDev B = a.blk[b];
+// one cell's share; returns its contribution to dJ/dKn
+__device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, int I, int J, const double* FLx,
+                                           const double* FRx, const double* FLy, const double* FRy) {
   double Pb[NV] = {0}, Ub[NV] = {0}, U[NV], P0[NV];
   double knb = 0.0;
   const bool ring = I == 0 || J == 0 || I == B.nxp - 1 || J == B.nyp - 1;
@@ -222,6 +235,16 @@ __global__ void __launch_bounds__(128, 4) adj_cells(AdjArgs a, long long ncell, 
 #pragma unroll
     for (int m = 0; m < NV; m++) a.lx[i + m * B.plane] += Ub[m];
   }
+  return knb;
+}
+
+__global__ void __launch_bounds__(128, 4) adj_cells(AdjArgs a, long long nthr, const double* FLx,
+                                                    const double* FRx, const double* FLy, const double* FRy) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b, I, J;
+  double knb = 0.0;
+  // threads past a block's edge stay for the warp sum below
+  if (k < nthr && locate(a.blk, a.nblk, k, b, I, J)) knb = cell_adj(a, a.blk[b], I, J, FLx, FRx, FLy, FRy);
   // the Kn derivative: warp sum, one atomic per warp
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) knb += __shfl_xor_sync(0xffffffffu, knb, o);
@@ -251,12 +274,12 @@ __global__ void adj_ghosts(const BlockDev* __restrict__ blk, const GhostEntry* _
 // each CTA writes its partial sum (fixed order: warp shuffles, then the warps in
 // order), so J does not depend on scheduling and finite differences of it are clean
 __global__ void adj_functional(const BlockDev* __restrict__ blk, int nblk, const double* x, double* l,
-                               long long ncell, double* part) {
+                               long long nthr, double* part) {
   __shared__ double ws[4];
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, Jj;
   double jv = 0.0;
-  if (k < ncell && locate(blk, nblk, k, b, I, Jj)) {
+  if (k < nthr && locate(blk, nblk, k, b, I, Jj)) {
     const BlockDev B = blk[b];
     if (inner(B, I, Jj)) {
       double U[NV], P[NV], Pb[NV] = {0}, Ub[NV] = {0};
@@ -293,17 +316,13 @@ __global__ void sum_partials(const double* part, int n, double* J) {
   }
 }
 
-cudaError_t adjoint_stage(const AdjArgs& a0, long long ncell, double* FLx, double* FRx, double* FLy,
+cudaError_t adjoint_stage(const AdjArgs& a0, long long nthr, double* FLx, double* FRx, double* FLy,
                           double* FRy, cudaStream_t s) {
   const int T = 128;
-  const unsigned G = (unsigned)((ncell + T - 1) / T);
-  adj_prims<<<G, T, 0, s>>>(a0, ncell);
-  AdjArgs a = a0;
-  a.FL = FLx; a.FR = FRx;
-  adj_faces<<<G, T, 0, s>>>(a, ncell, 1);
-  a.FL = FLy; a.FR = FRy;
-  adj_faces<<<G, T, 0, s>>>(a, ncell, 2);
-  adj_cells<<<G, T, 0, s>>>(a0, ncell, FLx, FRx, FLy, FRy);
+  const unsigned G = (unsigned)(nthr / T);
+  adj_prims<<<G, T, 0, s>>>(a0, nthr);
+  adj_faces<<<G, T, 0, s>>>(a0, nthr, FLx, FRx, FLy, FRy);
+  adj_cells<<<G, T, 0, s>>>(a0, nthr, FLx, FRx, FLy, FRy);
   return cudaGetLastError();
 }
 
@@ -313,11 +332,11 @@ cudaError_t adjoint_ghosts(const BlockDev* blk, const GhostEntry* map, int n, do
   return cudaGetLastError();
 }
 
-// part: (ncell + 127) / 128 doubles of scratch
-cudaError_t adjoint_functional(const BlockDev* blk, int nblk, const double* x, double* l, long long ncell,
+// nthr: 128 threads per 32 x 4 tile of every block; part: nthr / 128 doubles of scratch
+cudaError_t adjoint_functional(const BlockDev* blk, int nblk, const double* x, double* l, long long nthr,
                                double* part, double* J, cudaStream_t s) {
-  const unsigned G = (unsigned)((ncell + 127) / 128);
-  adj_functional<<<G, 128, 0, s>>>(blk, nblk, x, l, ncell, part);
+  const unsigned G = (unsigned)(nthr / 128);
+  adj_functional<<<G, 128, 0, s>>>(blk, nblk, x, l, nthr, part);
   sum_partials<<<1, 256, 0, s>>>(part, (int)G, J);
   return cudaGetLastError();
 }

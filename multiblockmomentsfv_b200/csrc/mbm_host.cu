@@ -934,9 +934,10 @@ extern "C" int mbm_trace_case(mbm_ctx* c, int k, double* rec, int cap, int* n) {
 // Discrete adjoint of a Steps run (hand-written reverse of Update and SetBoundary,
 // mbm_adjoint.cu), dt frozen from the forward run, checkpoints every k steps.
 
-static long long ncells(mbm_ctx* c) {
+// threads of an adjoint launch: one per cell, in 128-thread tiles of 32 x 4 cells per block
+static long long adj_threads(mbm_ctx* c) {
   long long n = 0;
-  for (auto& d : c->hblk) n += (long long)d.nxp * d.nyp;
+  for (auto& d : c->hblk) n += 128LL * ((d.nxp + 31) / 32) * ((d.nyp + 3) / 4);
   return n;
 }
 
@@ -944,7 +945,7 @@ static int adj_alloc(mbm_ctx* c, int nsteps, int every) {
   if (!c->adj_buf[0])
     for (int k = 0; k < 8; k++) CK(cudaMalloc(&c->adj_buf[k], sizeof(double) * c->layer_elems));
   if (!c->adj_scal) CK(cudaMalloc(&c->adj_scal, sizeof(double) * 2));
-  if (!c->adj_part) CK(cudaMalloc(&c->adj_part, sizeof(double) * ((ncells(c) + 127) / 128)));
+  if (!c->adj_part) CK(cudaMalloc(&c->adj_part, sizeof(double) * ((adj_threads(c) + 127) / 128)));
   if (nsteps > c->adj_nsteps || every != c->adj_every) {
     cudaFree(c->adj_ckpt);
     cudaFree(c->adj_seg);
@@ -993,7 +994,7 @@ static int adj_step(mbm_ctx* c, const double* Dn, const double* Tn, double dt, d
   const size_t bytes = sizeof(double) * c->layer_elems;
   double* lamT = c->adj_buf[2];
   double* P = c->adj_buf[3];
-  const long long nc = ncells(c);
+  const long long nc = adj_threads(c);
   const CaseDev& h = c->hcase[0];
   CK(cudaMemsetAsync(lamT, 0, bytes, c->stream));
   CK(cudaMemsetAsync(lam_next, 0, bytes, c->stream));
@@ -1066,7 +1067,7 @@ extern "C" int mbm_adjoint_run(mbm_ctx* c, double* t, int nsteps, int every, dou
   double* lam2 = c->adj_buf[1];
   CK(cudaMemsetAsync(c->adj_scal, 0, sizeof(double) * 2, c->stream));
   CK(cudaMemsetAsync(lam, 0, bytes, c->stream));
-  CK(adjoint_functional(c->dblk, c->nblk, c->buf[h.cur], lam, ncells(c), c->adj_part, c->adj_scal + 1, c->stream));
+  CK(adjoint_functional(c->dblk, c->nblk, c->buf[h.cur], lam, adj_threads(c), c->adj_part, c->adj_scal + 1, c->stream));
   // reverse sweep over segments [s*every, min((s+1)*every, n))
   const int cur0 = h.cur;
   if ((st = frozen_begin(c))) return st;
@@ -1146,9 +1147,9 @@ extern "C" int mbm_replay(mbm_ctx* c, const double* dts, int n, double* J) {
   if (J) {
     if (!c->adj_buf[0]) CK(cudaMalloc(&c->adj_buf[0], sizeof(double) * c->layer_elems));
     if (!c->adj_scal) CK(cudaMalloc(&c->adj_scal, sizeof(double) * 2));
-    if (!c->adj_part) CK(cudaMalloc(&c->adj_part, sizeof(double) * ((ncells(c) + 127) / 128)));
+    if (!c->adj_part) CK(cudaMalloc(&c->adj_part, sizeof(double) * ((adj_threads(c) + 127) / 128)));
     CK(cudaMemsetAsync(c->adj_scal, 0, sizeof(double) * 2, c->stream));
-    CK(adjoint_functional(c->dblk, c->nblk, c->buf[cur], c->adj_buf[0], ncells(c), c->adj_part, c->adj_scal + 1,
+    CK(adjoint_functional(c->dblk, c->nblk, c->buf[cur], c->adj_buf[0], adj_threads(c), c->adj_part, c->adj_scal + 1,
                           c->stream));
     double sc[2];
     CK(cudaMemcpyAsync(sc, c->adj_scal, sizeof sc, cudaMemcpyDeviceToHost, c->stream));

@@ -79,8 +79,6 @@ struct AdjArgs {       // one stage of the discrete adjoint (mbm_adjoint.cu)
   double* lx;            // += adjoint of the stage input (all cells)
   double* ld0;           // += adjoint of Data0 (stage 2)
   double* P;             // projected primitives of the stage input (layer layout)
-  double* FL;            // adjoint of the left/lower state of each face, at its left/lower cell
-  double* FR;            // adjoint of the right/upper state
   double* knb;           // += dJ/dKn
   double dt, Kn, F;
   int limiter, heun;
