@@ -244,6 +244,88 @@ def adjoint_leg(a, local, stream):
             "forward_ms": ms[0], "adjoint_ms": ms[1], "ratio": ms[1] / ms[0], "J": J, "dJ_dKn": gK}
 
 
+def run_sharded(a, rank, world, local):
+    """--shard: ONE case split over the ranks by block (strong scaling): the square
+    [-1,1]^2 at 2048 x 2048 cells as 2 x 2 blocks of 1024^2 (4 x 4 blocks of 512^2
+    beyond 4 ranks), blocks to ranks by cell count, one exchange of the ghost strips
+    per stage (NCCL point-to-point) and a max-reduction of the CFL per attempt."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from multiblockmomentsfv_b200 import blockfile as bf
+    from multiblockmomentsfv_b200 import scenario as sc
+    from multiblockmomentsfv_b200 import sharded as sh
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    side = 2 if world <= 4 else 4
+    d = bf.quadrant_deck(2 * a.n // side, Kn=0.01, R13=1.0, nblocks_side=side)
+    scn = sc.Scenario.seeded_quadrant(a.seed)
+    owner = sh.owners_by_cells(d, world)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        part = sh.ShardPart(d, owner, world, rank, scn, device=local, stream=stream.cuda_stream, mode=a.mode)
+        ex = sh.DistExchange() if world > 1 else sh.LocalExchange()
+        sh.initialise([part], scn, ex)
+        t, _, _ = sh.steps([part], ex, 0.0, 0.3, max_steps=a.warmup)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clk:
+            e0.record(stream)
+            t, n, r = sh.steps([part], ex, t, 0.3, max_steps=a.steps)
+            e1.record(stream)
+            stream.synchronize()
+        ms = e0.elapsed_time(e1)
+        v = torch.tensor([ms], device="cuda")
+        if world > 1:
+            dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        ms_max = float(v[0])
+        cells = d.full_grid_size
+        value = cells * n / (ms_max / 1e3)
+        # end to end: host state of the owned blocks up, one Steps call, down
+        own = [g for g in part.blocks]
+        host = {g: torch.empty((d.blocks[g].nyp, d.blocks[g].nxp, 9), dtype=torch.float64, pin_memory=True)
+                for g in own}
+        for g in own:
+            host[g].numpy()[:] = part.download(0, g)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for g in own:
+            part.upload(0, g, host[g].numpy())
+        sh.boundary([part], ex, 0)
+        t, ne, _ = sh.steps([part], ex, t, 0.3, max_steps=a.e2e_steps)
+        for g in own:
+            host[g].numpy()[:] = part.download(0, g)
+        f1.record(stream)
+        stream.synchronize()
+        v = torch.tensor([f0.elapsed_time(f1)], device="cuda")
+        if world > 1:
+            dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        e2e_value = cells * ne / (float(v[0]) / 1e3)
+        hb = sum(x.numel() * 8 for x in host.values())
+        part.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": n,
+            "warmup": a.warmup, "ms_per_step": ms_max / max(1, n), "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": f"synthetic: seeded quadrant state (seed {a.seed})",
+            "config": {"workload": f"one case split by block: [-1,1]^2 at {2 * a.n}^2 cells as {side}x{side} blocks, "
+                                   f"Kn=0.01, harmonic, CFL 0.95, FP64, {a.mode} mode", "mode": a.mode,
+                       "cells": cells, "owner": owner, "rejected_attempts": r,
+                       "parallelism": f"block sharding x{world} (ghost strips by NCCL point-to-point, CFL max-reduce)"},
+            "roofline": None,
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": hb / max(1, ne),
+                    "d2h_bytes_per_step": hb / max(1, ne), "steps_per_call": ne, "calls": 1},
+            "gpu_launches": 8 * (n + r), "clocks": clk.summary(), "cpu_baseline": None}), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -263,6 +345,8 @@ def main():
     ap.add_argument("--adjoint-every", type=int, default=20)
     ap.add_argument("--mode", default="fast", choices=["fast", "exact"],
                     help="stage-kernel arithmetic: fast (within 1e-10 / 1e-8 of the reference) or exact (bitwise)")
+    ap.add_argument("--shard", action="store_true",
+                    help="split ONE case over the ranks by block (strong scaling) instead of replicas")
     ap.add_argument("--exact-steps", type=int, default=100,
                     help="steps of the bitwise-mode comparison line when --mode fast (0 = skip)")
     a = ap.parse_args()
@@ -274,6 +358,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         run_reference(a, rank)
+        return
+    if a.shard:
+        run_sharded(a, rank, world, local)
         return
 
     import torch

@@ -164,6 +164,53 @@ int mbm_attempts(mbm_ctx *ctx, int *attempts);
  * reference, whose loop runs on through non-finite values. */
 int mbm_case_status(mbm_ctx *ctx, int *status, int n);
 
+/* ---- One case split over ranks by block (one process per GPU) ----------------
+ * No counterpart in the reference, which runs every block in one process.  Each
+ * rank owns whole blocks (owner[b] = rank of block b, the same table on every
+ * rank).  A ghost cell whose source cell is on another rank is filled from a
+ * receive buffer; the caller moves the send buffers' segments to the peers'
+ * receive buffers (e.g. NCCL send/recv) between mbm_shard_pack and mbm_shard_fill,
+ * ordered after the pack on the context's stream, and replaces the CFL scalar by
+ * its maximum over the ranks between mbm_shard_cfl and mbm_shard_control.  The
+ * Steps loop of one call, every rank in lockstep:
+ *   mbm_shard_begin; while (!done) { stage(0); pack(TMP); exchange; fill(TMP);
+ *   stage(1); pack(NEW); exchange; fill(NEW); cfl; max-reduce; control(&done) }
+ *   mbm_shard_end.
+ * Results equal the unsplit context's bit for bit (same map, same arithmetic;
+ * the maximum is order-free).  The initial ghost fill is pack(DATA), exchange,
+ * fill(DATA).  The single-context calls (mbm_steps, mbm_update, mbm_set_boundary,
+ * mbm_time_update, the adjoint) refuse a sharded context. */
+
+/* The exchange plan of one rank, on the host (no device needed): cells sent to and
+ * received from each rank (send_counts, recv_counts: nranks entries each); up to
+ * cap entries of send_cells (global block, cell J*(nx+6)+I) and recv_cells (global
+ * destination block, destination cell, wall flips: 1 = x, 2 = y), peers in rank
+ * order. */
+int mbm_shard_plan(const mbm_block_desc *blocks, int nblocks, const int *owner, int nranks, int rank,
+                   int *send_counts, int *recv_counts, int *send_cells, int *recv_cells, int cap);
+
+/* A context holding the blocks of `rank` (numbered in their global order). */
+int mbm_create_sharded(const mbm_block_desc *blocks, int nblocks, const int *owner, int nranks, int rank,
+                       const mbm_params *params, mbm_ctx **ctx);
+
+/* Cells per peer and the device buffers: send and receive (9 doubles per cell,
+ * peers in rank order) and the CFL scalar (1 double). */
+int mbm_shard_buffers(mbm_ctx *ctx, int *send_counts, int *recv_counts, int nranks, double **send,
+                      double **recv, double **cfl);
+
+/* Dirichlet ghost values (as mbm_set_dirichlet) of edge `side` of global block
+ * `block`: every rank sets those of all blocks, since a corner ghost cell can take
+ * its value from another rank's Dirichlet edge. */
+int mbm_shard_set_dirichlet(mbm_ctx *ctx, int block, int side, const double *values);
+
+int mbm_shard_begin(mbm_ctx *ctx, double t, double tend, double CFLmax, double CFLreg, int max_steps);
+int mbm_shard_stage(mbm_ctx *ctx, int heun);          /* Heun stage 1 (DATA -> TMP) or 2 (-> NEW) */
+int mbm_shard_pack(mbm_ctx *ctx, int layer);          /* this rank's cells other ranks need */
+int mbm_shard_fill(mbm_ctx *ctx, int layer);          /* SetBoundary of the layer, remote cells received */
+int mbm_shard_cfl(mbm_ctx *ctx);                      /* this rank's CFL of the attempt -> the scalar */
+int mbm_shard_control(mbm_ctx *ctx, int *done);       /* accept/reject with the scalar; waits */
+int mbm_shard_end(mbm_ctx *ctx, double *t, int *nsteps, int *nrej);
+
 /* Launch configuration in use: rows per warp work item (picked by the autotuner
  * when mbm_params.segment_rows is 0), work items per stage, CTAs of the persistent
  * stage grid. */

@@ -24,6 +24,9 @@ EXPORTS = (
     "mbm_create_batch", "mbm_steps_batch", "mbm_trace_case", "mbm_stage_noalloc",
     "mbm_adjoint_run", "mbm_replay", "mbm_set_physics", "mbm_output_fields",
     "mbm_ghost_map", "mbm_strerror", "mbm_last_error", "mbm_version",
+    "mbm_shard_plan", "mbm_create_sharded", "mbm_shard_buffers", "mbm_shard_set_dirichlet",
+    "mbm_shard_begin", "mbm_shard_stage",
+    "mbm_shard_pack", "mbm_shard_fill", "mbm_shard_cfl", "mbm_shard_control", "mbm_shard_end",
 )
 
 
@@ -81,6 +84,18 @@ def lib(path: str = None):
     L.mbm_trace.argtypes = [vp, dp, C.c_int, P(C.c_int)]
     L.mbm_attempts.argtypes = [vp, P(C.c_int)]
     L.mbm_case_status.argtypes = [vp, P(C.c_int), C.c_int]
+    ip = P(C.c_int)
+    L.mbm_shard_plan.argtypes = [P(BlockDesc), C.c_int, ip, C.c_int, C.c_int, ip, ip, ip, ip, C.c_int]
+    L.mbm_create_sharded.argtypes = [P(BlockDesc), C.c_int, ip, C.c_int, C.c_int, P(Params), P(vp)]
+    L.mbm_shard_buffers.argtypes = [vp, ip, ip, C.c_int, P(vp), P(vp), P(vp)]
+    L.mbm_shard_set_dirichlet.argtypes = [vp, C.c_int, C.c_int, dp]
+    L.mbm_shard_begin.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]
+    L.mbm_shard_stage.argtypes = [vp, C.c_int]
+    L.mbm_shard_pack.argtypes = [vp, C.c_int]
+    L.mbm_shard_fill.argtypes = [vp, C.c_int]
+    L.mbm_shard_cfl.argtypes = [vp]
+    L.mbm_shard_control.argtypes = [vp, ip]
+    L.mbm_shard_end.argtypes = [vp, dp, ip, ip]
     L.mbm_config.argtypes = [vp, P(C.c_int), P(C.c_int), P(C.c_int)]
     L.mbm_create_batch.argtypes = [P(BlockDesc), C.c_int, P(CaseDesc), C.c_int, P(Params), P(vp)]
     L.mbm_steps_batch.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_int, P(C.c_int), P(C.c_int)]

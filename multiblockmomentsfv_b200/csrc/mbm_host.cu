@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <array>
 #include <thread>
 #include <vector>
 
@@ -28,7 +29,14 @@ cudaError_t launch_stage(int lim, const StageArgs& a, int grid, cudaStream_t s);
 int stage_ctas_per_sm();
 }
 cudaError_t launch_ghost(const BlockDev* blk, const CaseDev* cases, const GhostEntry* map, int n,
-                         double* const buf[3], const double* dirichlet, int sel, cudaStream_t s);
+                         double* const buf[3], const double* dirichlet, int sel, cudaStream_t s,
+                         const double* recv = nullptr);
+cudaError_t launch_shard_pack(const BlockDev* blk, const CaseDev* cases, const int2* list, int n,
+                              double* const buf[3], int sel, double* send, cudaStream_t s);
+cudaError_t launch_shard_cfl(const CaseDev* cases, const BlockDev* blk, int nblk, unsigned long long* lam,
+                             double* out, cudaStream_t s);
+cudaError_t launch_control_ext(CaseDev* cases, const BlockDev* blk, unsigned long long* lam, double* trace,
+                               int* queues, const double* cfl_ext, cudaStream_t s);
 cudaError_t launch_control(CaseDev* cases, int ncases, const BlockDev* blk, unsigned long long* lam,
                            double* trace, int* queues, cudaGraphConditionalHandle h, int use_handle,
                            cudaStream_t s);
@@ -98,6 +106,15 @@ struct mbm_ctx {
   bool host_loop = false;           // MBM_HOST_LOOP=1: drive the step loop from the host
   bool adjoint = false;             // graph body records checkpoints and dt (mbm_params.adjoint)
   bool fast = false;                // MBM_MODE_FAST: the fastmath stage kernel
+  // a case split over ranks by block (mbm_create_sharded)
+  bool sharded = false;
+  std::vector<int> send_counts, recv_counts;
+  int nsend = 0, nrecv = 0;
+  int2* dsend_list = nullptr;
+  double* shard_send = nullptr;
+  double* shard_recv = nullptr;
+  double* shard_cfl = nullptr;
+  std::vector<int> shard_dir_off, shard_nt;   // Dirichlet rows of every block's edges (whole table)
   // adjoint work space (allocated on first use)
   double* adj_buf[8] = {nullptr};   // two adjoint layers, primitives, 4 face-adjoint layers, spare
   double* adj_ckpt = nullptr;
@@ -184,7 +201,7 @@ static int validate(const mbm_block_desc* b, int n, std::string& why, int lo = 0
 // race-free and its result equals the sequential sweeps bit for bit.
 namespace {
 struct Sym { int kind, blk, cell, flags; };   // kind 0 cell, 1 Dirichlet row, 2 unknown
-struct Resolved { int dst_blk, dst_cell, src, src_blk, flags; };
+struct Resolved { int dst_blk, dst_cell, src, src_blk, flags, remote = -1; };   // remote: receive index
 }  // namespace
 
 static int resolve_ghosts(const mbm_block_desc* B, int nb, std::vector<Resolved>& out,
@@ -438,9 +455,20 @@ static int autotune(mbm_ctx* c) {
   return set_segments(c, best);
 }
 
+// exchange plan of one rank of a case split over ranks by block (mbm_create_sharded)
+struct ShardSetup {
+  std::vector<int> send_counts, recv_counts;          // cells per peer rank
+  std::vector<std::array<int, 2>> send;               // (local block, cell J*nxp+I), peers in rank order
+  std::vector<int> dir_off, nt;                       // Dirichlet rows and edge lengths, [global block][side]
+};
+
+static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vector<int>& blk_case,
+                       const mbm_case_desc* cases, int ncases, const mbm_params* params,
+                       const std::vector<Resolved>& res, const std::vector<int>& dir_off, int ndir,
+                       const ShardSetup* shard, mbm_ctx** out);
+
 extern "C" int mbm_create_batch(const mbm_block_desc* blocks, int nblocks, const mbm_case_desc* cases,
                                 int ncases, const mbm_params* params, mbm_ctx** out) {
-  mbm_ctx* c = nullptr;
   if (!out || !params || !cases || ncases < 1) return fail(nullptr, MBM_EINVAL, "null argument");
   *out = nullptr;
   std::string why;
@@ -476,6 +504,17 @@ extern "C" int mbm_create_batch(const mbm_block_desc* blocks, int nblocks, const
   int ndir = 0;
   if (resolve_ghosts(glob.data(), nblocks, res, dir_off, ndir, why) != MBM_OK)
     return fail(nullptr, MBM_EINVAL, why);
+  return create_impl(glob, blk_case, cases, ncases, params, res, dir_off, ndir, nullptr, out);
+}
+
+// the context proper, from a block table whose ghost map is resolved; shard: the
+// exchange plan of a case split over ranks (nullptr otherwise)
+static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vector<int>& blk_case,
+                       const mbm_case_desc* cases, int ncases, const mbm_params* params,
+                       const std::vector<Resolved>& res, const std::vector<int>& dir_off, int ndir,
+                       const ShardSetup* shard, mbm_ctx** out) {
+  mbm_ctx* c = nullptr;
+  const int nblocks = (int)glob.size();
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(nullptr, MBM_ENODEV, "no CUDA device");
   if (params->device < 0 || params->device >= ndev) return fail(nullptr, MBM_EINVAL, "bad device ordinal");
@@ -546,6 +585,12 @@ extern "C" int mbm_create_batch(const mbm_block_desc* blocks, int nblocks, const
     GhostEntry e;
     e.dst_blk = r.dst_blk;
     e.dst = (r.dst_cell / D.nxp) * D.pitch + r.dst_cell % D.nxp + 1;
+    if (r.remote >= 0) {
+      e.src = r.remote;
+      e.src_blk_flags = (r.flags << 16) | GHOST_REMOTE;
+      gm[i] = e;
+      continue;
+    }
     if (r.src >= 0) {
       const BlockDev& S = c->hblk[r.src_blk];
       e.src = (r.src / S.nxp) * S.pitch + r.src % S.nxp + 1;
@@ -596,6 +641,35 @@ extern "C" int mbm_create_batch(const mbm_block_desc* blocks, int nblocks, const
   {
     int st0 = params->segment_rows > 0 ? set_segments(c, std::max(8, params->segment_rows)) : autotune(c);
     if (st0) return bail(st0);
+  }
+
+  if (shard) {   // exchange buffers, send list, the CFL scalar; the step loop is driven per phase
+    c->sharded = true;
+    c->shard_dir_off = shard->dir_off;
+    c->shard_nt = shard->nt;
+    c->send_counts = shard->send_counts;
+    c->recv_counts = shard->recv_counts;
+    c->nsend = (int)shard->send.size();
+    c->nrecv = 0;
+    for (int v : shard->recv_counts) c->nrecv += v;
+    std::vector<int2> sl(shard->send.size());
+    for (size_t i = 0; i < sl.size(); i++) {
+      const BlockDev& d = c->hblk[shard->send[i][0]];
+      const int cell = shard->send[i][1];
+      sl[i] = make_int2(shard->send[i][0], (cell / d.nxp) * d.pitch + cell % d.nxp + 1);
+    }
+    CKC(cudaMalloc(&c->dsend_list, sizeof(int2) * std::max<size_t>(1, sl.size())));
+    if (!sl.empty())
+      CKC(cudaMemcpyAsync(c->dsend_list, sl.data(), sizeof(int2) * sl.size(), cudaMemcpyHostToDevice, c->stream));
+    CKC(cudaMalloc(&c->shard_send, sizeof(double) * NV * std::max(1, c->nsend)));
+    CKC(cudaMalloc(&c->shard_recv, sizeof(double) * NV * std::max(1, c->nrecv)));
+    CKC(cudaMemsetAsync(c->shard_recv, 0, sizeof(double) * NV * std::max(1, c->nrecv), c->stream));
+    CKC(cudaMalloc(&c->shard_cfl, sizeof(double)));
+    CKC(cudaMemsetAsync(c->shard_cfl, 0, sizeof(double), c->stream));
+    int st = wait_stream(c);
+    if (st != MBM_OK) return bail(st);
+    *out = c;
+    return MBM_OK;
   }
 
   // the step loop: while (any case live) { stage 1; fill TMP; stage 2; fill NEW; control }
@@ -661,6 +735,10 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   cudaFree(c->adj_dtrep);
   cudaFree(c->adj_part);
   cudaFree(c->adj_scal);
+  cudaFree(c->dsend_list);
+  cudaFree(c->shard_send);
+  cudaFree(c->shard_recv);
+  cudaFree(c->shard_cfl);
   cudaFree(c->dtrace);
   cudaFree(c->dcfl);
   if (c->hcfl) cudaFreeHost(c->hcfl);
@@ -731,6 +809,7 @@ static void live_all(mbm_ctx* c, double dt, double t) {
 }
 
 extern "C" int mbm_set_boundary(mbm_ctx* c, int layer, double t) {
+  if (c && c->sharded) return fail(c, MBM_EINVAL, "mbm_set_boundary: the context holds part of a sharded case (mbm_shard_*)");
   (void)t;   // Dirichlet values are the host-set table; the reference's states are steady
   if (!c || bad_layer(layer)) return fail(c, MBM_EINVAL, "mbm_set_boundary: bad argument");
   CK(cudaSetDevice(c->device));
@@ -754,6 +833,7 @@ static int run_stage(mbm_ctx* c, int out_layer, int in_layer, int d0_layer, int 
 
 extern "C" int mbm_update(mbm_ctx* c, int out_layer, int in_layer, int data0_layer, double dt,
                           double t, int heun, double* cfl) {
+  if (c && c->sharded) return fail(c, MBM_EINVAL, "mbm_update: the context holds part of a sharded case (mbm_shard_*)");
   if (!c || bad_layer(out_layer) || bad_layer(in_layer) || bad_layer(data0_layer) || (heun != 0 && heun != 1) ||
       out_layer == in_layer || out_layer == data0_layer)
     return fail(c, MBM_EINVAL, "mbm_update: bad argument");
@@ -765,6 +845,7 @@ extern "C" int mbm_update(mbm_ctx* c, int out_layer, int in_layer, int data0_lay
 }
 
 extern "C" int mbm_time_update(mbm_ctx* c, double dt, double t, double* cfl) {
+  if (c && c->sharded) return fail(c, MBM_EINVAL, "mbm_time_update: the context holds part of a sharded case (mbm_shard_*)");
   if (!c) return fail(c, MBM_EINVAL, "mbm_time_update: null context");
   std::vector<double> v(c->nblk);
   double c1 = 0.0, c2 = 0.0;
@@ -784,6 +865,7 @@ extern "C" int mbm_time_update(mbm_ctx* c, double dt, double t, double* cfl) {
 // ends when every case is done (t >= tend, max_steps reached, or a failure).
 extern "C" int mbm_steps_batch(mbm_ctx* c, double* t, const double* tend, double CFLmax, double CFLreg,
                                int max_steps, int* nsteps, int* nrej) {
+  if (c && c->sharded) return fail(c, MBM_EINVAL, "mbm_steps: the context holds part of a sharded case (mbm_shard_*)");
   if (!c || !t || !tend || max_steps < 0) return fail(c, MBM_EINVAL, "mbm_steps: bad argument");
   CK(cudaSetDevice(c->device));
   bool any = false;
@@ -1030,6 +1112,7 @@ static int adj_step(mbm_ctx* c, const double* Dn, const double* Tn, double dt, d
 
 extern "C" int mbm_adjoint_run(mbm_ctx* c, double* t, int nsteps, int every, double CFLreg, double* J,
                                double* grad, double* grad_Kn, double* dts_out, double* ms) {
+  if (c && c->sharded) return fail(c, MBM_EINVAL, "mbm_adjoint_run: the context holds part of a sharded case (mbm_shard_*)");
   if (!c || !t || nsteps < 1 || every < 1 || c->ncase != 1) return fail(c, MBM_EINVAL, "mbm_adjoint_run: bad argument");
   if (!c->adjoint) return fail(c, MBM_EINVAL, "mbm_adjoint_run: context created without mbm_params.adjoint");
   CK(cudaSetDevice(c->device));
@@ -1123,6 +1206,7 @@ extern "C" int mbm_adjoint_run(mbm_ctx* c, double* t, int nsteps, int every, dou
 // frozen-dt forward: n Heun steps of DATA with the given dt values, no controller;
 // *J (may be NULL) receives the heat-flux functional of the result
 extern "C" int mbm_replay(mbm_ctx* c, const double* dts, int n, double* J) {
+  if (c && c->sharded) return fail(c, MBM_EINVAL, "mbm_replay: the context holds part of a sharded case (mbm_shard_*)");
   if (!c || (n > 0 && !dts) || n < 0 || c->ncase != 1) return fail(c, MBM_EINVAL, "mbm_replay: bad argument");
   CK(cudaSetDevice(c->device));
   CaseDev& h = c->hcase[0];
@@ -1167,6 +1251,256 @@ extern "C" int mbm_set_physics(mbm_ctx* c, double Kn, double F) {
     c->hcase[k].F = F;
   }
   return push_cases(c);
+}
+
+// ---------------------------------------------------------------- sharding --
+// One case split over ranks by block.  Every rank resolves the ghost map of the whole
+// block table (the same on every rank) and keeps the entries of its own blocks; an
+// entry whose source cell lies on another rank reads it from a receive buffer.  The
+// cells rank p sends to rank r are those entries of r's blocks with a source on p,
+// in the order of the global map, so both sides agree on the order without talking.
+static int shard_split(const mbm_block_desc* blocks, int nblocks, const int* owner, int nranks, int rank,
+                       std::vector<Resolved>& res, std::vector<int>& dir_off, int& ndir,
+                       std::vector<std::array<int, 2>>& send, std::vector<std::array<int, 3>>& recv,
+                       std::vector<int>& send_counts, std::vector<int>& recv_counts, std::string& why) {
+  if (!owner || nranks < 1 || rank < 0 || rank >= nranks) { why = "bad owner table, rank or rank count"; return MBM_EINVAL; }
+  if (validate(blocks, nblocks, why) != MBM_OK) return MBM_EINVAL;
+  for (int b = 0; b < nblocks; b++)
+    if (owner[b] < 0 || owner[b] >= nranks) { why = "block " + std::to_string(b + 1) + ": owner out of range"; return MBM_EINVAL; }
+  if (resolve_ghosts(blocks, nblocks, res, dir_off, ndir, why) != MBM_OK) return MBM_EINVAL;
+  std::vector<std::vector<std::array<int, 2>>> S(nranks);
+  std::vector<std::vector<std::array<int, 3>>> R(nranks);
+  for (Resolved& r : res) {
+    if (r.src < 0) continue;
+    const int od = owner[r.dst_blk], os = owner[r.src_blk];
+    if (od == os) continue;
+    if (os == rank) S[od].push_back({r.src_blk, r.src});
+    if (od == rank) {
+      r.remote = (int)R[os].size();   // index within the peer's segment, offset added below
+      R[os].push_back({r.dst_blk, r.dst_cell, r.flags});
+    }
+  }
+  send_counts.assign(nranks, 0);
+  recv_counts.assign(nranks, 0);
+  std::vector<int> roff(nranks, 0);
+  send.clear();
+  recv.clear();
+  for (int p = 0; p < nranks; p++) {
+    send_counts[p] = (int)S[p].size();
+    recv_counts[p] = (int)R[p].size();
+    roff[p] = (int)recv.size();
+    send.insert(send.end(), S[p].begin(), S[p].end());
+    recv.insert(recv.end(), R[p].begin(), R[p].end());
+  }
+  for (Resolved& r : res)
+    if (r.remote >= 0) r.remote += roff[owner[r.src_blk]];
+  return MBM_OK;
+}
+
+extern "C" int mbm_shard_plan(const mbm_block_desc* blocks, int nblocks, const int* owner, int nranks, int rank,
+                              int* send_counts, int* recv_counts, int* send_cells, int* recv_cells, int cap) {
+  std::string why;
+  std::vector<Resolved> res;
+  std::vector<int> dir_off, sc, rc;
+  std::vector<std::array<int, 2>> send;
+  std::vector<std::array<int, 3>> recv;
+  int ndir = 0;
+  if (shard_split(blocks, nblocks, owner, nranks, rank, res, dir_off, ndir, send, recv, sc, rc, why) != MBM_OK)
+    return fail(nullptr, MBM_EINVAL, why);
+  for (int p = 0; p < nranks; p++) {
+    if (send_counts) send_counts[p] = sc[p];
+    if (recv_counts) recv_counts[p] = rc[p];
+  }
+  for (int i = 0; i < (int)send.size() && i < cap && send_cells; i++) {
+    send_cells[2 * i] = send[i][0];
+    send_cells[2 * i + 1] = send[i][1];
+  }
+  for (int i = 0; i < (int)recv.size() && i < cap && recv_cells; i++)
+    for (int k = 0; k < 3; k++) recv_cells[3 * i + k] = recv[i][k];
+  return MBM_OK;
+}
+
+extern "C" int mbm_create_sharded(const mbm_block_desc* blocks, int nblocks, const int* owner, int nranks,
+                                  int rank, const mbm_params* params, mbm_ctx** out) {
+  if (!out || !params) return fail(nullptr, MBM_EINVAL, "null argument");
+  *out = nullptr;
+  if (params->mode != MBM_MODE_EXACT && params->mode != MBM_MODE_FAST)
+    return fail(nullptr, MBM_EINVAL, "unknown arithmetic mode");
+  if (params->limiter < 0 || params->limiter > 4) return fail(nullptr, MBM_EINVAL, "limiter code must be 0..4");
+  if (!(params->Kn > 1e-100 && params->Kn < 1e100)) return fail(nullptr, MBM_EINVAL, "Kn must be in (1e-100, 1e100)");
+  std::string why;
+  std::vector<Resolved> res;
+  std::vector<int> dir_off, sc, rc;
+  std::vector<std::array<int, 2>> send;
+  std::vector<std::array<int, 3>> recv;
+  int ndir = 0;
+  if (shard_split(blocks, nblocks, owner, nranks, rank, res, dir_off, ndir, send, recv, sc, rc, why) != MBM_OK)
+    return fail(nullptr, MBM_EINVAL, why);
+  std::vector<int> g2l(nblocks, -1);
+  std::vector<mbm_block_desc> loc;
+  for (int b = 0; b < nblocks; b++)
+    if (owner[b] == rank) {
+      g2l[b] = (int)loc.size();
+      loc.push_back(blocks[b]);
+    }
+  if (loc.empty()) return fail(nullptr, MBM_EINVAL, "rank " + std::to_string(rank) + " owns no block");
+  for (auto& d : loc)   // the resolved map carries the interfaces; codes of remote partners read as open
+    for (int s = 0; s < 4; s++)
+      if (d.bc[s] > 0) d.bc[s] = g2l[d.bc[s] - 1] >= 0 ? g2l[d.bc[s] - 1] + 1 : 0;
+  std::vector<Resolved> lres;
+  for (const Resolved& r : res) {
+    if (g2l[r.dst_blk] < 0) continue;
+    Resolved q = r;
+    q.dst_blk = g2l[r.dst_blk];
+    if (r.src >= 0 && r.remote < 0) q.src_blk = g2l[r.src_blk];
+    lres.push_back(q);
+  }
+  std::vector<int> ldir((size_t)loc.size() * 4, -1);
+  for (int b = 0; b < nblocks; b++)
+    if (g2l[b] >= 0)
+      for (int s = 0; s < 4; s++) ldir[(size_t)g2l[b] * 4 + s] = dir_off[(size_t)b * 4 + s];
+  ShardSetup setup;
+  setup.dir_off = dir_off;
+  for (int b = 0; b < nblocks; b++)
+    for (int s2 = 0; s2 < 4; s2++) setup.nt.push_back(s2 < 2 ? blocks[b].ny + 2 * NG : blocks[b].nx + 2 * NG);
+  setup.send_counts = sc;
+  setup.recv_counts = rc;
+  for (const auto& e : send) setup.send.push_back({g2l[e[0]], e[1]});
+  mbm_case_desc one;
+  one.first_block = 0;
+  one.nblocks = (int)loc.size();
+  one.Kn = params->Kn;
+  one.F = params->F;
+  one.limiter = params->limiter;
+  std::vector<int> blk_case(loc.size(), 0);
+  return create_impl(loc, blk_case, &one, 1, params, lres, ldir, ndir, &setup, out);
+}
+
+static int need_shard(mbm_ctx* c, const char* what) {
+  if (!c) return fail(nullptr, MBM_EINVAL, std::string(what) + ": null context");
+  if (!c->sharded) return fail(c, MBM_EINVAL, std::string(what) + ": context is not sharded");
+  return MBM_OK;
+}
+
+extern "C" int mbm_shard_buffers(mbm_ctx* c, int* send_counts, int* recv_counts, int nranks, double** send,
+                                 double** recv, double** cfl) {
+  int st = need_shard(c, "mbm_shard_buffers");
+  if (st) return st;
+  if (nranks != (int)c->send_counts.size()) return fail(c, MBM_EINVAL, "mbm_shard_buffers: wrong rank count");
+  for (int p = 0; p < nranks; p++) {
+    if (send_counts) send_counts[p] = c->send_counts[p];
+    if (recv_counts) recv_counts[p] = c->recv_counts[p];
+  }
+  if (send) *send = c->shard_send;
+  if (recv) *recv = c->shard_recv;
+  if (cfl) *cfl = c->shard_cfl;
+  return MBM_OK;
+}
+
+// Dirichlet values of any block's edge: a ghost cell at a corner may take its value
+// from the Dirichlet row of a block another rank owns, so every rank holds them all
+extern "C" int mbm_shard_set_dirichlet(mbm_ctx* c, int block, int side, const double* values) {
+  int st = need_shard(c, "mbm_shard_set_dirichlet");
+  if (st) return st;
+  if (!values || block < 0 || block * 4 >= (int)c->shard_dir_off.size() || side < 0 || side > 3)
+    return fail(c, MBM_EINVAL, "mbm_shard_set_dirichlet: bad argument");
+  const int row = c->shard_dir_off[block * 4 + side];
+  if (row < 0) return fail(c, MBM_EINVAL, "mbm_shard_set_dirichlet: edge is not a Dirichlet edge");
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(c->ddir + (size_t)row * NV, values, sizeof(double) * c->shard_nt[block * 4 + side] * NG * NV,
+                     cudaMemcpyHostToDevice, c->stream));
+  return wait_stream(c);
+}
+
+extern "C" int mbm_shard_begin(mbm_ctx* c, double t, double tend, double CFLmax, double CFLreg, int max_steps) {
+  int st = need_shard(c, "mbm_shard_begin");
+  if (st) return st;
+  if (max_steps < 0) return fail(c, MBM_EINVAL, "mbm_shard_begin: bad argument");
+  CK(cudaSetDevice(c->device));
+  CaseDev& h = c->hcase[0];
+  h.t = t;
+  h.tend = tend;
+  h.dt = 0.0001;               // DT_INITIAL, reset on every call (src/Main.c:28,193)
+  h.CFLmax = CFLmax;
+  h.CFLreg = CFLreg;
+  h.nstep = h.nrej = h.attempts = 0;
+  h.step_cap = max_steps;
+  h.status = 0;
+  h.nonfinite = 0;
+  h.trace_n = 0;
+  h.show_every = c->prm.show_every;
+  h.max_attempts = c->prm.max_attempts;
+  h.done = (t < tend) ? 0 : 1;
+  return push_cases(c);
+}
+
+extern "C" int mbm_shard_stage(mbm_ctx* c, int heun) {
+  int st = need_shard(c, "mbm_shard_stage");
+  if (st) return st;
+  if (heun != 0 && heun != 1) return fail(c, MBM_EINVAL, "mbm_shard_stage: bad argument");
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemsetAsync(c->dqueue + heun * 5, 0, sizeof(int) * 5, c->stream));
+  CK(launch_stages(c, heun, heun ? SEL_TMP : SEL_CUR, SEL_CUR, heun ? SEL_OTHER : SEL_TMP));
+  return MBM_OK;
+}
+
+extern "C" int mbm_shard_pack(mbm_ctx* c, int layer) {
+  int st = need_shard(c, "mbm_shard_pack");
+  if (st) return st;
+  if (bad_layer(layer)) return fail(c, MBM_EINVAL, "mbm_shard_pack: bad layer");
+  CK(cudaSetDevice(c->device));
+  CK(launch_shard_pack(c->dblk, c->dcase, c->dsend_list, c->nsend, c->buf, layer_sel(layer), c->shard_send, c->stream));
+  return MBM_OK;
+}
+
+extern "C" int mbm_shard_fill(mbm_ctx* c, int layer) {
+  int st = need_shard(c, "mbm_shard_fill");
+  if (st) return st;
+  if (bad_layer(layer)) return fail(c, MBM_EINVAL, "mbm_shard_fill: bad layer");
+  CK(cudaSetDevice(c->device));
+  const bool was_done = c->hcase[0].done != 0;
+  if (was_done) {              // the fill kernel skips finished cases: the initial fill runs between calls
+    c->hcase[0].done = 0;
+    if ((st = push_cases(c))) return st;
+  }
+  CK(launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, layer_sel(layer), c->stream,
+                  c->shard_recv));
+  if (was_done) {
+    c->hcase[0].done = 1;
+    if ((st = push_cases(c))) return st;
+  }
+  return MBM_OK;
+}
+
+extern "C" int mbm_shard_cfl(mbm_ctx* c) {
+  int st = need_shard(c, "mbm_shard_cfl");
+  if (st) return st;
+  CK(cudaSetDevice(c->device));
+  CK(launch_shard_cfl(c->dcase, c->dblk, c->nblk, c->dlam, c->shard_cfl, c->stream));
+  return MBM_OK;
+}
+
+extern "C" int mbm_shard_control(mbm_ctx* c, int* done) {
+  int st = need_shard(c, "mbm_shard_control");
+  if (st) return st;
+  CK(cudaSetDevice(c->device));
+  CK(launch_control_ext(c->dcase, c->dblk, c->dlam, c->dtrace, c->dqueue, c->shard_cfl, c->stream));
+  CK(cudaMemcpyAsync(c->hcase, c->dcase, sizeof(CaseDev), cudaMemcpyDeviceToHost, c->stream));
+  if ((st = wait_stream(c))) return st;
+  if (done) *done = c->hcase[0].done;
+  return MBM_OK;
+}
+
+extern "C" int mbm_shard_end(mbm_ctx* c, double* t, int* nsteps, int* nrej) {
+  int st = need_shard(c, "mbm_shard_end");
+  if (st) return st;
+  const CaseDev& h = c->hcase[0];
+  if (t) *t = h.t;
+  if (nsteps) *nsteps = h.nstep;
+  if (nrej) *nrej = h.nrej;
+  if (h.status == 2) return fail(c, MBM_ENONFINITE, "a stage wrote NaN or infinity, or CFL or dt became non-finite");
+  if (h.status == 5) return fail(c, MBM_ESTEPLIMIT, "step attempts exceeded max_attempts");
+  return MBM_OK;
 }
 
 // ------------------------------------------------------------------- misc --

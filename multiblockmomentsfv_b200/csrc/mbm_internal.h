@@ -36,11 +36,13 @@ struct Work {          // one warp strip segment: columns [I0, I0+28), face rows
   int blk, I0, J0, J1;
 };
 
+constexpr int GHOST_REMOTE = 1 << 18;   // src_blk_flags: src indexes the receive buffer
+
 struct GhostEntry {    // final value of one ghost cell after the two-sweep fill
   int dst_blk;
   int dst;             // element index (J*pitch + I + 1) in block dst_blk
   int src;             // >= 0: element index in block src_blk; < 0: Dirichlet row -(src+1)
-  int src_blk_flags;   // src_blk | (x-wall flip << 16) | (y-wall flip << 17)
+  int src_blk_flags;   // src_blk | (x-wall flip << 16) | (y-wall flip << 17) | GHOST_REMOTE
 };
 
 struct CaseDev {       // per-case step controller (src/Main.c:189-244)

@@ -18,7 +18,7 @@ using namespace bitwise;    // the output conversion uses the bitwise Primitive
 __global__ void ghost_kernel(const BlockDev* __restrict__ blk, const CaseDev* __restrict__ cases,
                              const GhostEntry* __restrict__ map, int n, double* buf0,
                              double* buf1, double* buf2, const double* __restrict__ dirichlet,
-                             int sel) {
+                             const double* __restrict__ recv, int sel) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const GhostEntry e = map[i];
@@ -33,7 +33,9 @@ __global__ void ghost_kernel(const BlockDev* __restrict__ blk, const CaseDev* __
 #pragma unroll
   for (int m = 0; m < NV; m++) {
     double v;
-    if (e.src >= 0) {
+    if (e.src_blk_flags & GHOST_REMOTE) {          // a source cell on another rank
+      v = recv[(size_t)e.src * NV + m];
+    } else if (e.src >= 0) {
       const BlockDev S = blk[sblk];
       v = layer[S.off + m * S.plane + e.src];
     } else {
@@ -50,7 +52,7 @@ __global__ void ghost_kernel(const BlockDev* __restrict__ blk, const CaseDev* __
 // CFL > CFLmax, else accept, swap DATA/NEW and advance t; next dt = dt*CFLreg/CFL.
 __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __restrict__ blk,
                                unsigned long long* lam, double* trace, int* queues,
-                               cudaGraphConditionalHandle h, int use_handle) {
+                               cudaGraphConditionalHandle h, int use_handle, const double* cfl_ext) {
   if (threadIdx.x < 10) queues[threadIdx.x] = 0;  // work counters [stage][limiter]
   int live = 0;
   for (int c = threadIdx.x; c < ncases; c += blockDim.x) {
@@ -69,7 +71,8 @@ __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __res
       if (v2 > cfl2) cfl2 = v2;
       for (int k = 0; k < 6; k++) s[k] = 0ull;
     }
-    const double cfl = rmax(cfl1, rmax(cfl2, 0.0));
+    // a case split over ranks brings the max over all ranks (single-case contexts)
+    const double cfl = cfl_ext ? *cfl_ext : rmax(cfl1, rmax(cfl2, 0.0));
     cs.cfl_last = cfl;
     cs.attempts++;
     if (cs.nonfinite) {       // a stage wrote a NaN or infinity: stop before accepting it
@@ -213,19 +216,79 @@ __global__ void planes_to_aos(const double* __restrict__ src, double* __restrict
   aos[k] = src[m * plane + (long long)J * pitch + I + 1];
 }
 
+// ------------------------------------------------------------------ sharding --
+// A case split over ranks by block.  pack: the cells other ranks' ghost cells copy,
+// gathered from the selected layer into the send buffer (9 values per cell, in the
+// plan's order); the ghost kernel reads them back from the receive buffer.
+__global__ void shard_pack_kernel(const BlockDev* __restrict__ blk, const CaseDev* __restrict__ cases,
+                                  const int2* __restrict__ list, int n, const double* buf0,
+                                  const double* buf1, const double* buf2, int sel, double* __restrict__ send) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * NV) return;
+  const int i = (int)(t / NV), m = (int)(t - (long long)i * NV);
+  const int2 e = list[i];
+  const BlockDev B = blk[e.x];
+  const double* bufs[3] = {buf0, buf1, buf2};
+  const double* layer = bufs[phys_layer(sel, cases[0].cur)];
+  send[t] = layer[B.off + m * B.plane + e.y];
+}
+
+// this rank's share of the CFL of one attempt (case 0, all local blocks), into *out;
+// the per-block maxima are cleared as the controller would
+__global__ void shard_cfl_kernel(const CaseDev* __restrict__ cases, const BlockDev* __restrict__ blk, int nblk,
+                                 unsigned long long* lam, double* out) {
+  if (threadIdx.x != 0) return;
+  const double dt = cases[0].dt;
+  double cfl1 = 0.0, cfl2 = 0.0;
+  for (int b = 0; b < nblk; b++) {
+    unsigned long long* s = lam + (size_t)b * 6;
+    const double dx = blk[b].dx, dy = blk[b].dy;
+    const double v1 = dt * __longlong_as_double(s[0]) / dx + dt * __longlong_as_double(s[1]) / dy +
+                      __longlong_as_double(s[2]);
+    const double v2 = dt * __longlong_as_double(s[3]) / dx + dt * __longlong_as_double(s[4]) / dy +
+                      __longlong_as_double(s[5]);
+    if (v1 > cfl1) cfl1 = v1;
+    if (v2 > cfl2) cfl2 = v2;
+    for (int k = 0; k < 6; k++) s[k] = 0ull;
+  }
+  // a non-finite write on this rank makes every rank reject the attempt and stop
+  *out = cases[0].nonfinite ? __longlong_as_double(0x7ff0000000000000LL) : rmax(cfl1, rmax(cfl2, 0.0));
+}
+
+cudaError_t launch_shard_pack(const BlockDev* blk, const CaseDev* cases, const int2* list, int n,
+                              double* const buf[3], int sel, double* send, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  shard_pack_kernel<<<(unsigned)(((long long)n * NV + 255) / 256), 256, 0, s>>>(blk, cases, list, n, buf[0], buf[1],
+                                                                                buf[2], sel, send);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shard_cfl(const CaseDev* cases, const BlockDev* blk, int nblk, unsigned long long* lam,
+                             double* out, cudaStream_t s) {
+  shard_cfl_kernel<<<1, 32, 0, s>>>(cases, blk, nblk, lam, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_control_ext(CaseDev* cases, const BlockDev* blk, unsigned long long* lam, double* trace,
+                               int* queues, const double* cfl_ext, cudaStream_t s) {
+  control_kernel<<<1, 256, 0, s>>>(cases, 1, blk, lam, trace, queues, cudaGraphConditionalHandle{}, 0, cfl_ext);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ launchers --
 cudaError_t launch_ghost(const BlockDev* blk, const CaseDev* cases, const GhostEntry* map, int n,
-                         double* const buf[3], const double* dirichlet, int sel, cudaStream_t s) {
+                         double* const buf[3], const double* dirichlet, int sel, cudaStream_t s,
+                         const double* recv) {
   if (n <= 0) return cudaSuccess;
   ghost_kernel<<<(n + 127) / 128, 128, 0, s>>>(blk, cases, map, n, buf[0], buf[1], buf[2],
-                                               dirichlet, sel);
+                                               dirichlet, recv, sel);
   return cudaGetLastError();
 }
 
 cudaError_t launch_control(CaseDev* cases, int ncases, const BlockDev* blk, unsigned long long* lam,
                            double* trace, int* queues, cudaGraphConditionalHandle h, int use_handle,
                            cudaStream_t s) {
-  control_kernel<<<1, 256, 0, s>>>(cases, ncases, blk, lam, trace, queues, h, use_handle);
+  control_kernel<<<1, 256, 0, s>>>(cases, ncases, blk, lam, trace, queues, h, use_handle, nullptr);
   return cudaGetLastError();
 }
 
