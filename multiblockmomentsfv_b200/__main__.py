@@ -3,12 +3,14 @@
     python -m multiblockmomentsfv_b200 -bfile cases/squareSmall.txt -out runs/ss [-double]
         [-refine n] [-CFL x] [-Kn x] [-R13 x] [-limiter name] [-sfile file]
         [-scenario riemann2d|ffs|quadrant:SEED|uniform:r,u,v,th] [-device k] [-fast]
+        [-restart-faithful]
 
 Flags keep the reference's meaning and its quirks: numeric overrides pass through
 ``float`` (src/tools.c:38-46), -refine precedes the block file, and -sfile reloads the
 first zones of a result pair into L_DATA with the reference's mapping of the stored
 fields (src/Mesh.c:391-476: the stored pressure p goes where the temperature belongs and
-P_ij where T_ij belongs).  -scenario picks the initial/Dirichlet state that the
+P_ij where T_ij belongs; -restart-faithful reads the last level with the correct
+mapping instead).  -scenario picks the initial/Dirichlet state that the
 reference hard-codes in src/Scenario.c (default riemann2d).  -fast runs the stage
 kernel in fast arithmetic (MBM_MODE_FAST: within 1e-10 of the reference per field after
 one step, 1e-8 at the end time, not bitwise).
@@ -43,17 +45,28 @@ def _scenario(spec: str) -> sc.Scenario:
     return sc.Scenario.named(spec)
 
 
-def load_restart(deck: bf.Deck, path: str):
+def load_restart(deck: bf.Deck, path: str, faithful: bool = False):
     """LoadData (src/Mesh.c:391-476): the first len(blocks) zones fill the interior
-    plus one ghost ring of L_DATA; the remaining cells stay zero."""
+    plus one ghost ring of L_DATA; the remaining cells stay zero.  Like the reference,
+    the stored pressure goes where the temperature belongs and P_ij where T_ij belongs,
+    and the first zones of a multi-level file are its t = 0 level.
+
+    faithful=True (CLI -restart-faithful) reads the last time level instead and maps
+    the fields to the state they came from: theta = T, T_ij = P_ij / rho."""
     zones, _ = out.read(path)
+    nb = len(deck.blocks)
+    sel = zones[len(zones) - nb:] if faithful else zones[:nb]
     layers = []
-    for b, z in zip(deck.blocks, zones[:len(deck.blocks)]):
+    for b, z in zip(deck.blocks, sel):
         U = np.zeros((b.nyp, b.nxp, bf.NV))
         vals = z["values"].reshape(b.nx + 2, b.ny + 2, 10)      # x outer, y inner
         P = np.empty((b.nx + 2, b.ny + 2, bf.NV))
         P[..., 0:3] = vals[..., 0:3]
-        P[..., 3:7] = vals[..., 4:8]
+        if faithful:
+            P[..., 3] = vals[..., 3]
+            P[..., 4:7] = vals[..., 5:8] / vals[..., 0:1]
+        else:
+            P[..., 3:7] = vals[..., 4:8]
         P[..., 7:9] = vals[..., 8:10]
         rho, v1, v2, th = P[..., 0], P[..., 1], P[..., 2], P[..., 3]
         vs = v1 * v1 + v2 * v2
@@ -91,7 +104,7 @@ def main(argv=None) -> int:
     mode = "fast" if "-fast" in argv else "exact"
     with sv.Solver(deck, scn, device=device, mode=mode) as s:
         if sfile:
-            for b, U in enumerate(load_restart(deck, sfile)):
+            for b, U in enumerate(load_restart(deck, sfile, faithful="-restart-faithful" in argv)):
                 s.upload(sv.L_DATA, b, U)
             s.set_boundary(sv.L_DATA, 0.0)
         else:

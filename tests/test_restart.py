@@ -1,0 +1,56 @@
+"""The restart loader (-sfile): the reference's LoadData mapping by default, and the
+opt-in faithful mapping (-restart-faithful) that reloads the last written level into
+the state it came from.  Host only."""
+import numpy as np
+
+import helpers as H
+from multiblockmomentsfv_b200 import __main__ as cli
+from multiblockmomentsfv_b200 import blockfile as bf
+from multiblockmomentsfv_b200 import output
+
+
+def _levels(d, seed):
+    rng = np.random.default_rng(seed)
+    return [[H.random_layer(rng, b) for b in d.blocks] for _ in range(2)]
+
+
+def _ring(U, b):
+    return U[2:b.ny + 4, 2:b.nx + 4]
+
+
+def test_faithful_restart_reloads_the_last_level(tmp_path):
+    d = H.deck("squareSmall")
+    lv = _levels(d, 1)
+    w = output.Writer(str(tmp_path), d, "Riemann2D", single=False)
+    w.write(lv[0], 0.0, -1)
+    w.write(lv[1], 0.1, 5)
+    got = cli.load_restart(d, w.base, faithful=True)
+    for b, blk in enumerate(d.blocks):
+        a, ref = _ring(got[b], blk), _ring(lv[1][b], blk)
+        assert np.allclose(a, ref, rtol=1e-12, atol=1e-14), np.abs(a - ref).max()
+        # outside the interior plus one ghost ring the layer stays zero (set by the ghost fill)
+        assert not got[b][0].any() and not got[b][:, 0].any()
+
+
+def test_default_restart_keeps_the_references_mapping(tmp_path):
+    """The reference's LoadData puts the stored p where theta belongs and P_ij where
+    T_ij belongs, and reads the first level: a state at rest with rho = 2, theta = 1
+    comes back with theta = p = 2 and T_ii = P_ii = 2."""
+    d = H.deck("squareSmall")
+    lv = []
+    for b in d.blocks:
+        U = np.zeros((b.nyp, b.nxp, bf.NV))
+        U[..., 0] = 2.0
+        U[..., 3] = 1.5 * 2.0          # E = 3/2 rho theta
+        U[..., 4] = 2.0                # rho T11
+        U[..., 6] = 2.0
+        lv.append(U)
+    w = output.Writer(str(tmp_path), d, "Riemann2D", single=False)
+    w.write(lv, 0.0, -1)
+    w.write([U * 1.1 for U in lv], 0.1, 5)
+    got = cli.load_restart(d, w.base)
+    for b, blk in enumerate(d.blocks):
+        a = _ring(got[b], blk)
+        assert np.allclose(a[..., 0], 2.0)
+        assert np.allclose(a[..., 3], 1.5 * 2.0 * 2.0)      # theta taken as p = 2
+        assert np.allclose(a[..., 4], 2.0 * 2.0)            # T11 taken as P11 = 2
