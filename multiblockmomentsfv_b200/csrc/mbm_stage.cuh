@@ -82,14 +82,32 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   // and the y face (r-2 | r-1), then finishes row J = r-2 (x face, update).
   const int rs = w.J0 >= 2 ? w.J0 - 2 : w.J0 - 1;
   int s0 = rs % 3;                 // window slot of row r
+  // Stage 1 loads the moments of row r+1 while it works on row r (nine registers,
+  // which stage 2, holding Data0 as well, cannot spare without spilling).
+  constexpr bool PREFETCH = HEUN == 0;
+  double Un[NV];
+  if (PREFETCH) {
+    const bool ok = col_in && rs >= 0 && rs < nyp;
+    if (ok) load_cell(in, plane, (long long)rs * pitch + C + 1, Un);
+    else benign(Un);
+  }
   for (int r = rs; r <= w.J1 + 1; r++) {
     const int sm1 = s0 == 0 ? 2 : s0 - 1, sm2 = sm1 == 0 ? 2 : sm1 - 1;
     // (a) projected primitives of row r: Aux.Prim (src/Main.c:314-336)
     {
       double U[NV], Q[NV];
       const bool ok = col_in && r >= 0 && r < nyp;
-      if (ok) load_cell(in, plane, (long long)r * pitch + C + 1, U);
-      else benign(U);
+      if (PREFETCH) {
+#pragma unroll
+        for (int n = 0; n < NV; n++) U[n] = Un[n];
+        const bool okn = col_in && r + 1 >= 0 && r + 1 < nyp;
+        if (okn) load_cell(in, plane, (long long)(r + 1) * pitch + C + 1, Un);
+        else benign(Un);
+      } else if (ok) {
+        load_cell(in, plane, (long long)r * pitch + C + 1, U);
+      } else {
+        benign(U);
+      }
       primitive(U, Q);
       if (ok && col_cell && r >= 1 && r <= nyp - 2) {
         const double c = relax_cfl<2 * HEUN>(Q, dt, Kn);
