@@ -204,6 +204,8 @@ __device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, 
   if (anyP) {     // Aux = relax(Primitive(U), 2H+1) off the ring (ring cells never reach a face)
     mbm_adj::relax_p_adj(P0, Pb, Qb, &knb, a.dt, a.Kn, 2 * a.heun + 1);
   }
+  const long long ic = cidx(B, I, J);
+  double Vb[NV] = {0};
   if (inner(B, I, J)) {
     // update term R: Conservative(relax(Primitive(X), 2H)) [+ Conservative(relax(Primitive(D0), -1))]
     const double s = a.heun ? 0.5 : 1.0;
@@ -214,26 +216,30 @@ __device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, 
     mbm_adj::cons_adj(Q, Rb, Cb);
     mbm_adj::relax_p_adj(P0, Cb, Qb, &knb, a.dt, a.Kn, 2 * a.heun);
     if (a.heun) {
-      double V[NV], W[NV], Q2[NV], C2[NV] = {0}, Pd[NV] = {0}, Vb[NV] = {0};
+      double V[NV], W[NV], Q2[NV], C2[NV] = {0}, Pd[NV] = {0};
       load9(a.d0, B, I, J, V);
       mbm_adj::prim(V, W);
       mbm_adj::relax_p(W, Q2, a.dt, a.Kn, a.F, -1);
       mbm_adj::cons_adj(Q2, Rb, C2);
       mbm_adj::relax_p_adj(W, C2, Pd, &knb, a.dt, a.Kn, -1);
       mbm_adj::prim_adj(V, Pd, Vb);
-      const long long i = cidx(B, I, J);
-#pragma unroll
-      for (int m = 0; m < NV; m++) a.ld0[i + m * B.plane] += Vb[m];
     }
   }
   bool anyQ = false;
 #pragma unroll
   for (int m = 0; m < NV; m++) anyQ = anyQ || Qb[m] != 0.0;
-  if (anyQ) {     // cells no stage output depends on may hold no state (zero density)
-    mbm_adj::prim_adj(U, Qb, Ub);
-    const long long i = cidx(B, I, J);
+  if (anyQ) mbm_adj::prim_adj(U, Qb, Ub);   // cells no stage output depends on may hold no state
+  // stage 2 starts both adjoint layers (every cell written: no clearing pass), stage 1
+  // adds to the layer stage 2 started
+  if (a.heun) {
 #pragma unroll
-    for (int m = 0; m < NV; m++) a.lx[i + m * B.plane] += Ub[m];
+    for (int m = 0; m < NV; m++) {
+      a.lx[ic + m * B.plane] = Ub[m];
+      a.ld0[ic + m * B.plane] = Vb[m];
+    }
+  } else if (anyQ) {
+#pragma unroll
+    for (int m = 0; m < NV; m++) a.lx[ic + m * B.plane] += Ub[m];
   }
   return knb;
 }

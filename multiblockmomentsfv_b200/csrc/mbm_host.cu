@@ -1073,13 +1073,11 @@ static int frozen_step(mbm_ctx* c, const double* in, double* out, const double* 
 // reverse of one step: lam (adjoint of D_{n+1}, interior) -> lam_next (adjoint of
 // D_n); Tn = stage 1 of D_n with its ghost fill
 static int adj_step(mbm_ctx* c, const double* Dn, const double* Tn, double dt, double* lam, double* lam_next) {
-  const size_t bytes = sizeof(double) * c->layer_elems;
   double* lamT = c->adj_buf[2];
   double* P = c->adj_buf[3];
   const long long nc = adj_threads(c);
   const CaseDev& h = c->hcase[0];
-  CK(cudaMemsetAsync(lamT, 0, bytes, c->stream));
-  CK(cudaMemsetAsync(lam_next, 0, bytes, c->stream));
+  // no clearing: stage 2's cell pass writes every cell of lamT and lam_next
   AdjArgs a{};
   a.blk = c->dblk;
   a.nblk = c->nblk;
