@@ -27,6 +27,7 @@ EXPORTS = (
     "mbm_shard_plan", "mbm_create_sharded", "mbm_shard_buffers", "mbm_shard_set_dirichlet",
     "mbm_shard_begin", "mbm_shard_stage",
     "mbm_shard_pack", "mbm_shard_fill", "mbm_shard_cfl", "mbm_shard_control", "mbm_shard_end",
+    "mbm_fastmath_check",
 )
 
 
@@ -96,6 +97,7 @@ def lib(path: str = None):
     L.mbm_shard_cfl.argtypes = [vp]
     L.mbm_shard_control.argtypes = [vp, ip]
     L.mbm_shard_end.argtypes = [vp, dp, ip, ip]
+    L.mbm_fastmath_check.argtypes = [vp, C.c_int, vp]
     L.mbm_config.argtypes = [vp, P(C.c_int), P(C.c_int), P(C.c_int)]
     L.mbm_create_batch.argtypes = [P(BlockDesc), C.c_int, P(CaseDesc), C.c_int, P(Params), P(vp)]
     L.mbm_steps_batch.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_int, P(C.c_int), P(C.c_int)]
