@@ -18,7 +18,7 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libmbm_b200.so")
 
 SOURCES = ["mbm_host.cu", "mbm_kernels.cu", "mbm_stage_fast.cu", "mbm_noalloc.cu", "mbm_adjoint.cu"]
-HEADERS = ["mbm_internal.h", "mbm_math.cuh", "mbm_stage.cuh", "mbm_adjoint_math.cuh"]
+HEADERS = ["mbm_internal.h", "mbm_math.cuh", "mbm_stage.cuh", "mbm_adjoint_math.cuh", "mbm_newton.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

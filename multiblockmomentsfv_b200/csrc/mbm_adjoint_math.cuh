@@ -21,6 +21,10 @@
 
 #include <math.h>
 
+#ifdef __CUDACC__
+#include "mbm_newton.cuh"
+#endif
+
 #ifndef MBM_HD
 #ifdef __CUDACC__
 #define MBM_HD __host__ __device__ __forceinline__
@@ -33,13 +37,22 @@ namespace mbm_adj {
 
 constexpr int NV = 9;
 
-// 1/x: the correctly rounded reciprocal on the device, one multiply per quotient
-// after it (the derivatives need no bit-exact quotients)
+// 1/x and sqrt(x): on the device the Newton-refined hardware approximations
+// (mbm_newton.cuh; the derivatives need no bit-exact values), one multiply per
+// quotient after the reciprocal
 MBM_HD double rcp(double x) {
 #ifdef __CUDA_ARCH__
-  return __drcp_rn(x);
+  return mbm_newton::frcp(x);
 #else
   return 1.0 / x;
+#endif
+}
+
+MBM_HD double root(double x) {
+#ifdef __CUDA_ARCH__
+  return mbm_newton::fsqrt(x);
+#else
+  return sqrt(x);
 #endif
 }
 
@@ -176,7 +189,7 @@ MBM_HD double rdamp(double z, int flag, double* dz) {
 // relaxation in primitive form: P -> Q (ProductionsDirect's state, src/Flux.c:230-267)
 MBM_HD void relax_p(const double* P, double* Q, double dt, double Kn, double F, int flag) {
   const double r = P[0], th = P[3];
-  const double z = r * sqrt(th) * rcp(Kn) * dt;
+  const double z = r * root(th) * rcp(Kn) * dt;
   double dd;
   const double d1 = rdamp(z, flag, &dd);
   const double d2 = rdamp(2.0 / 3 * z, flag, &dd);
@@ -195,7 +208,7 @@ MBM_HD void relax_p(const double* P, double* Q, double dt, double Kn, double F, 
 MBM_HD void relax_p_adj(const double* P, const double* Qb, double* Pb, double* Knb, double dt, double Kn,
                         int flag) {
   const double r = P[0], th = P[3];
-  const double z = r * sqrt(th) * rcp(Kn) * dt;
+  const double z = r * root(th) * rcp(Kn) * dt;
   double r1, r2;
   const double d1 = rdamp(z, flag, &r1);
   const double d2 = rdamp(2.0 / 3 * z, flag, &r2);
@@ -317,7 +330,7 @@ MBM_HD void hll_p(const double* PL_, const double* PR_, double* flx, int dir) {
   double PL[NV], PR[NV], UL[NV], UR[NV], fL[NV], fR[NV];
   if (dir == 2) { swap_xy(PL_, PL); swap_xy(PR_, PR); }
   else for (int n = 0; n < NV; n++) { PL[n] = PL_[n]; PR[n] = PR_[n]; }
-  const double cL = 2.0 * sqrt(5.0 / 3 * PL[3]), cR = 2.0 * sqrt(5.0 / 3 * PR[3]);
+  const double cL = 2.0 * root(5.0 / 3 * PL[3]), cR = 2.0 * root(5.0 / 3 * PR[3]);
   cons(PL, UL); cons(PR, UR); gflux_x(PL, fL); gflux_x(PR, fR);
   const double lamL = (PL[1] - cL) < 0.0 ? PL[1] - cL : 0.0;
   const double lamR = (PR[1] + cR) > 0.0 ? PR[1] + cR : 0.0;
@@ -340,7 +353,7 @@ MBM_HD void hll_p_adj(const double* PL_, const double* PR_, const double* fb_, d
   double PL[NV], PR[NV], fb[NV], T[NV];
   if (dir == 2) { swap_xy(PL_, PL); swap_xy(PR_, PR); swap_xy(fb_, fb); }
   else for (int n = 0; n < NV; n++) { PL[n] = PL_[n]; PR[n] = PR_[n]; fb[n] = fb_[n]; }
-  const double cL = 2.0 * sqrt(5.0 / 3 * PL[3]), cR = 2.0 * sqrt(5.0 / 3 * PR[3]);
+  const double cL = 2.0 * root(5.0 / 3 * PL[3]), cR = 2.0 * root(5.0 / 3 * PR[3]);
   const bool aL = (PL[1] - cL) < 0.0, aR = (PR[1] + cR) > 0.0;
   const double lamL = aL ? PL[1] - cL : 0.0;
   const double lamR = aR ? PR[1] + cR : 0.0;

@@ -22,6 +22,7 @@
 #if MBM_FAST_ARITH
 #define MBM_HD __host__ __device__ __forceinline__
 #include "mbm_adjoint_math.cuh"   // primitive-form Conservative and Grad-13 flux
+#include "mbm_newton.cuh"
 #endif
 
 namespace mbm {
@@ -72,32 +73,10 @@ __device__ __forceinline__ double mk_div(double x, double y, double r) {
 __device__ __noinline__ double div_ieee(double x, double y) { return x / y; }
 
 // Reciprocal, square root and lone quotients.  Bitwise: IEEE division and sqrt.
-// Fast arithmetic: Newton-Raphson refinement of the hardware's approximate
-// reciprocal and reciprocal square root (PTX rcp.approx.ftz.f64, rsqrt.approx.ftz.f64)
-// -- the classical iterations r' = r + r(1 - y r) for 1/y and s' = s(3 - x s^2)/2
-// for 1/sqrt(x), then one correction q' = q + (x - q^2) s/2 of the root (Markstein;
-// Muller et al., Handbook of Floating-Point Arithmetic, 2nd ed., ch. 4-5).  Two steps
-// on the reciprocal and the root correction give the correctly rounded result on all
-// of 2e6 random operands over exponents -300..300 (mbm_fastmath_check, tested), at a
-// fraction of the cost of the IEEE-exact sequences; normal operands only (flush to
-// zero), positive for the root.
+// Fast arithmetic: the Newton-refined hardware approximations of mbm_newton.cuh.
 #if MBM_FAST_ARITH
-__device__ __forceinline__ double frcp(double y) {
-  double r;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(y));
-  double e = fma(-y, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-y, r, 1.0);
-  return fma(r, e, r);
-}
-__device__ __forceinline__ double fsqrt(double x) {
-  double s;
-  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(s) : "d"(x));
-  s = s * fma(-0.5 * x, s * s, 1.5);
-  const double q = x * s;                      // sqrt(x) to about 2^-46
-  const double e = fma(-q, q, x);              // its residual, exact
-  return x == 0.0 ? 0.0 : fma(0.5 * s, e, q);
-}
+using mbm_newton::frcp;
+using mbm_newton::fsqrt;
 __device__ __forceinline__ double fdiv(double x, double y) { return x * frcp(y); }
 #else
 __device__ __forceinline__ double fdiv(double x, double y) { return x / y; }
