@@ -57,3 +57,18 @@ def test_reference_host_with_gpu_steps(tmp_path, name, scenario, t_list, dt_out,
     ok, mx, msg = out.compare(a, b, 0.0, 0.0)
     assert ok and mx == 0.0, msg
     assert "(gpu)" in log_gpu or "Done after" in log_gpu
+
+
+def test_reference_host_with_fast_gpu_steps(tmp_path):
+    """MBM_MODE=fast in the drop-in: the reference's regression gate at its Float64
+    defaults (|a - b| <= 1e-10 + 1e-8 |b|) against the unmodified reference."""
+    deck = _deck(tmp_path, "square4", "0.1", "0.05")
+    os.environ["MBM_MODE"] = "fast"
+    try:
+        a, _ = _run("moments_b200", deck, str(tmp_path / "gpu"), "riemann2d")
+    finally:
+        del os.environ["MBM_MODE"]
+    b, _ = _run("moments", deck, str(tmp_path / "ref"), "riemann2d")
+    ok, mx, msg = out.compare(a, b)
+    assert ok, msg
+    assert mx > 0.0          # not the bitwise kernel
