@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "mbm_internal.h"
 #include "mbm_math.cuh"
 
@@ -45,7 +47,17 @@ struct WarpWindow {
   double P[3][NV][32];
   double lo[NV][32];
   double G[NV][32];
+  double D0[2][NV][32];   // stage 2: Data0 of the next two update rows (asynchronous copies)
 };
+
+// per-thread asynchronous 8-byte copy global -> shared (cp.async), and its groups
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 constexpr int STAGE_WARPS = 4;
 #ifndef STAGE_MIN_CTAS
 #define STAGE_MIN_CTAS 3   // CTAs per SM the register budget is sized for (168 registers)
@@ -85,6 +97,20 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   // Stage 1 loads the moments of row r+1 while it works on row r (nine registers,
   // which stage 2, holding Data0 as well, cannot spare without spilling).
   constexpr bool PREFETCH = HEUN == 0;
+  // Stage 2 copies Data0 of update row J (= r-2 at iteration r) into shared memory two
+  // iterations ahead, without registers: one group per row, committed even when empty
+  auto d0_fetch = [&](int Jn) {
+    if (HEUN == 1) {
+      if (col_out && Jn >= NG && Jn <= nyp - 1 - NG && Jn >= w.J0 && Jn < w.J1) {
+        const long long idx = (long long)Jn * pitch + C + 1;
+#pragma unroll
+        for (int n = 0; n < NV; n++) cp_async8(&win.D0[Jn & 1][n][lane], d0 + n * plane + idx);
+      }
+      cp_async_commit();
+    }
+  };
+  d0_fetch(rs - 2);
+  d0_fetch(rs - 1);
   double Un[NV];
   if (PREFETCH) {
     const bool ok = col_in && rs >= 0 && rs < nyp;
@@ -171,6 +197,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     }
     // (c) row J = r-2: x slope, x face C | C+1 (src/Main.c:346-347, 372-378), update
     const int J = r - 2;
+    if (HEUN == 1) cp_async_wait_one();     // this row's Data0 has landed
     if (J >= w.J0 && J < w.J1) {
       double P0[NV], Sx[NV], lo[NV], hi[NV], F[NV];
       bool xbad = false;
@@ -214,7 +241,8 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         relax<2 * HEUN>(Q, R, dt, Kn, Fx);
         if (HEUN == 1) {
           double R0[NV];
-          load_cell(d0, plane, idx, U);
+#pragma unroll
+          for (int n = 0; n < NV; n++) U[n] = win.D0[J & 1][n][lane];
           primitive(U, Q);
           relax<-1>(Q, R0, dt, Kn, Fx);
 #pragma unroll
@@ -237,8 +265,10 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
 #pragma unroll
       for (int n = 0; n < NV; n++) win.G[n][lane] = G[n];
     }
+    d0_fetch(r);                            // into the slot row J = r-2 has left
     s0 = s0 == 2 ? 0 : s0 + 1;
   }
+  if (HEUN == 1) cp_async_wait_all();       // nothing in flight past the work item
 
   // per-block maxima; the values are >= 0 (or NaN, which never passes a '>' test
   // above), so their bit patterns order like the values
@@ -261,9 +291,14 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
 // Persistent grid (as many CTAs as fit on the SMs); every warp takes the next work
 // item from a counter until the table is exhausted, so uneven blocks and the last
 // wave balance themselves.
+// the windows live in dynamic shared memory (STAGE_SMEM bytes, above the 48 KB a static
+// allocation may take)
+constexpr int STAGE_SMEM = (int)sizeof(WarpWindow) * STAGE_WARPS;
+
 template <int HEUN, int LIM>
 __global__ void __launch_bounds__(32 * STAGE_WARPS, STAGE_MIN_CTAS) stage_kernel(const StageArgs a) {
-  __shared__ WarpWindow win[STAGE_WARPS];
+  extern __shared__ __align__(16) unsigned char stage_smem[];
+  WarpWindow* win = reinterpret_cast<WarpWindow*>(stage_smem);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (;;) {
     int w = 0;
@@ -274,20 +309,41 @@ __global__ void __launch_bounds__(32 * STAGE_WARPS, STAGE_MIN_CTAS) stage_kernel
   }
 }
 
+template <int HEUN, int LIM>
+static void smem_attr() {
+  cudaFuncSetAttribute(stage_kernel<HEUN, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM);
+}
+
+// called at context creation (the device current), before any launch or graph capture:
+// allows the dynamic shared memory for every instantiation on this device, then asks
+// how many CTAs fit per SM
 int stage_ctas_per_sm() {
+  static std::mutex mu;
+  static unsigned long long done = 0;     // one bit per device ordinal < 64
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> g(mu);
+    const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
+    if (!bit || !(done & bit)) {
+      smem_attr<0, 0>(); smem_attr<0, 1>(); smem_attr<0, 2>(); smem_attr<0, 3>(); smem_attr<0, 4>();
+      smem_attr<1, 0>(); smem_attr<1, 1>(); smem_attr<1, 2>(); smem_attr<1, 3>(); smem_attr<1, 4>();
+      done |= bit;
+    }
+  }
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<1, 4>, 32 * STAGE_WARPS, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<1, 4>, 32 * STAGE_WARPS, STAGE_SMEM);
   return n > 0 ? n : 1;
 }
 
 template <int HEUN>
 static cudaError_t launch_stage_lim(int lim, const StageArgs& a, int grid, cudaStream_t s) {
   switch (lim) {
-    case 0: stage_kernel<HEUN, 0><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
-    case 1: stage_kernel<HEUN, 1><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
-    case 2: stage_kernel<HEUN, 2><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
-    case 3: stage_kernel<HEUN, 3><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
-    default: stage_kernel<HEUN, 4><<<grid, 32 * STAGE_WARPS, 0, s>>>(a); break;
+    case 0: stage_kernel<HEUN, 0><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
+    case 1: stage_kernel<HEUN, 1><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
+    case 2: stage_kernel<HEUN, 2><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
+    case 3: stage_kernel<HEUN, 3><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
+    default: stage_kernel<HEUN, 4><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
   }
   return cudaGetLastError();
 }
