@@ -145,26 +145,21 @@ def run_reference(a, rank):
     print(json.dumps(line), flush=True)
 
 
-def batched_leg(a, local, stream, rank):
-    """Many independent cases: one context advancing all of them in one CUDA-graph
-    loop (per-case dt, one persistent launch per limiter per stage) against the same
-    cases run one after another, each in its own context.  Device time (CUDA events)
-    of the step loops only; context creation and initial states are outside.  A case
-    that produces a non-finite value stops there in both arms (the unlimited
-    'average' slopes blow up on some quadrant states, in the reference too); the
-    throughput counts the steps each case took."""
+def _batch_vs_serial(cases, steps, local, stream, mode):
+    """Device time of one batched step loop over `cases` and of the same cases one
+    context each; returns (cell-updates batched, ms, cell-updates serial, ms, steps
+    per case batched, steps per case serial, statuses, graph attempts)."""
     import torch
     from multiblockmomentsfv_b200 import solver as sv
-    cases = sv.batch_workload(seed=a.seed + rank, ncases=a.batch_cases)
     cells = [d.full_grid_size for d, _ in cases]
     ev = lambda: torch.cuda.Event(enable_timing=True)
-    with sv.BatchSolver(cases, device=local, stream=stream.cuda_stream, mode=a.mode) as bs:
+    with sv.BatchSolver(cases, device=local, stream=stream.cuda_stream, mode=mode) as bs:
         bs.initialise()
         bs.steps(0.0, 10.0, max_steps=2, check=False)
         bs.initialise()
         e0, e1 = ev(), ev()
         e0.record(stream)
-        _, ns, _ = bs.steps(0.0, 10.0, max_steps=a.batch_steps, check=False)
+        _, ns, _ = bs.steps(0.0, 10.0, max_steps=steps, check=False)
         e1.record(stream)
         stream.synchronize()
         ms_b = e0.elapsed_time(e1)
@@ -173,26 +168,51 @@ def batched_leg(a, local, stream, rank):
     upd_b = float(sum(c * n for c, n in zip(cells, ns)))
     ms_s, upd_s, ns_serial = 0.0, 0.0, []
     for (d, scn), c in zip(cases, cells):
-        with sv.BatchSolver([(d, scn)], device=local, stream=stream.cuda_stream, mode=a.mode) as s1:
+        with sv.BatchSolver([(d, scn)], device=local, stream=stream.cuda_stream, mode=mode) as s1:
             s1.initialise()
             s1.steps(0.0, 10.0, max_steps=2, check=False)
             s1.initialise()
             e0, e1 = ev(), ev()
             e0.record(stream)
-            _, n1, _ = s1.steps(0.0, 10.0, max_steps=a.batch_steps, check=False)
+            _, n1, _ = s1.steps(0.0, 10.0, max_steps=steps, check=False)
             e1.record(stream)
             stream.synchronize()
             ms_s += e0.elapsed_time(e1)
             upd_s += c * int(n1[0])
             ns_serial.append(int(n1[0]))
-    failed = [{"case": k, "limiter": cases[k][0].limiter, "steps": int(ns[k])}
+    return upd_b, ms_b, upd_s, ms_s, [int(x) for x in ns], ns_serial, status, launches
+
+
+def batched_leg(a, local, stream, rank):
+    """Many independent cases: one context advancing all of them in one CUDA-graph
+    loop (per-case dt, one persistent launch per limiter per stage) against the same
+    cases run one after another, each in its own context.  Device time (CUDA events)
+    of the step loops only; context creation and initial states are outside.  A case
+    that produces a non-finite value stops there in both arms (the unlimited
+    'average' slopes blow up on some quadrant states, in the reference too); the
+    throughput counts the steps each case took.  The same comparison over the cases
+    of at most 4 x 384^2 cells shows the batching where launch latency, not the
+    stage kernel, bounds a case run alone."""
+    from multiblockmomentsfv_b200 import solver as sv
+    cases = sv.batch_workload(seed=a.seed + rank, ncases=a.batch_cases)
+    upd_b, ms_b, upd_s, ms_s, ns, ns_serial, status, launches = _batch_vs_serial(
+        cases, a.batch_steps, local, stream, a.mode)
+    small = [c for c in cases if c[0].full_grid_size <= 4 * 384 * 384]
+    sm = None
+    if small:
+        sb, smb, ss, sms, _, _, _, _ = _batch_vs_serial(small, a.batch_steps, local, stream, a.mode)
+        sm = {"cases": len(small), "value": sb / (smb / 1e3), "serial_value": ss / (sms / 1e3),
+              "ratio": (sb / smb) / (ss / sms), "ms": smb, "serial_ms": sms}
+    failed = [{"case": k, "limiter": cases[k][0].limiter, "steps": ns[k]}
               for k in range(len(cases)) if status[k] != 0]
-    return {"cases": len(cases), "steps_per_case": a.batch_steps, "cells": int(sum(cells)),
+    return {"cases": len(cases), "steps_per_case": a.batch_steps,
+            "cells": int(sum(d.full_grid_size for d, _ in cases)),
             "value": upd_b / (ms_b / 1e3), "serial_value": upd_s / (ms_s / 1e3),
             "ratio": (upd_b / ms_b) / (upd_s / ms_s), "unit": "cell-updates/s",
             "ms": ms_b, "serial_ms": ms_s, "graph_attempts": launches,
-            "same_steps_as_serial": [int(x) for x in ns] == ns_serial,
+            "same_steps_as_serial": ns == ns_serial,
             "stopped_nonfinite": failed,
+            "small_cases": sm,
             "workload": f"{len(cases)} seeded cases, 1-4 blocks of n x n, n ~ U{{64..1024}}, Kn log-U[1e-3,1e-1], "
                         "R13 in {0,1}, limiter ~ U{5}, quadrant state, open edges, "
                         f"{a.batch_steps} steps each, per-case dt; serial = the same cases one context and one "
