@@ -101,6 +101,9 @@ struct mbm_ctx {
   double* dcfl = nullptr;           // per-block stage CFL for mbm_update
   double* hcfl = nullptr;           // pinned
   cudaEvent_t ev = nullptr;
+  // limiter groups of one stage run concurrently: forked from `stream`, joined back
+  cudaStream_t aux[4] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[4] = {};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   bool host_loop = false;           // MBM_HOST_LOOP=1: drive the step loop from the host
@@ -341,9 +344,20 @@ static int set_segments(mbm_ctx* c, int seg) {
 }
 
 // one Heun stage of every block: one persistent launch per limiter group
+// (with several limiter groups, group k > 0 runs on aux stream k-1, so that one
+// group's CTAs fill the SMs another group's tail leaves idle)
 static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, int sel_out,
                                  double* const* bufs = nullptr) {
-  for (const LimGroup& g : c->groups) {
+  const int ng = (int)c->groups.size();
+  cudaError_t e0;
+  if (ng > 1) {
+    if ((e0 = cudaEventRecord(c->fork_ev, c->stream))) return e0;
+    for (int k = 1; k < ng; k++)
+      if ((e0 = cudaStreamWaitEvent(c->aux[k - 1], c->fork_ev, 0))) return e0;
+  }
+  for (int k = 0; k < ng; k++) {
+    const LimGroup& g = c->groups[k];
+    cudaStream_t st = k == 0 ? c->stream : c->aux[k - 1];
     StageArgs a{};
     a.blk = c->dblk;
     a.work = c->dwork + g.start;
@@ -354,9 +368,13 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
     a.queue = c->dqueue + heun * 5 + g.lim;
     a.sel_in = sel_in; a.sel_d0 = sel_d0; a.sel_out = sel_out;
     a.heun = heun;
-    cudaError_t e = c->fast ? fastmath::launch_stage(g.lim, a, g.grid, c->stream)
-                            : bitwise::launch_stage(g.lim, a, g.grid, c->stream);
+    cudaError_t e = c->fast ? fastmath::launch_stage(g.lim, a, g.grid, st)
+                            : bitwise::launch_stage(g.lim, a, g.grid, st);
     if (e != cudaSuccess) return e;
+  }
+  for (int k = 1; k < ng; k++) {
+    if ((e0 = cudaEventRecord(c->join_ev[k - 1], c->aux[k - 1]))) return e0;
+    if ((e0 = cudaStreamWaitEvent(c->stream, c->join_ev[k - 1], 0))) return e0;
   }
   return cudaSuccess;
 }
@@ -551,6 +569,11 @@ static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vecto
     c->own_stream = true;
   }
   CKC(cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming));
+  CKC(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+  for (int k = 0; k < 4; k++) {
+    CKC(cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking));
+    CKC(cudaEventCreateWithFlags(&c->join_ev[k], cudaEventDisableTiming));
+  }
 
   // block table and layer layout
   long long off = 0, max_cells = 0;
@@ -743,6 +766,11 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   cudaFree(c->dcfl);
   if (c->hcfl) cudaFreeHost(c->hcfl);
   if (c->ev) cudaEventDestroy(c->ev);
+  if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+  for (int k = 0; k < 4; k++) {
+    if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
+    if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
+  }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return MBM_OK;
