@@ -447,13 +447,14 @@ def main():
     ms2 = s.time_stage(1, dt, reps=5)
     achieved = BYTES_PER_CELL_UPDATE * cells / ((ms1 + ms2) / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = None
+    traffic, fp64 = None, None
     tp = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
             tj = json.load(f)
         if tj.get("cells_per_launch"):
             traffic = tj["dram_bytes_per_launch_per_cell"] * cells
+        fp64 = tj.get("fp64_pipe_active_pct")
 
     # end to end through the C ABI with host buffers: upload DATA (pinned host, array of
     # structs), one Steps() call of e2e-steps Heun steps, download DATA -- per call
@@ -514,6 +515,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "stage_kernel (Heun stage 1 + stage 2)",
+                         "fp64_pipe_active_pct_ncu": fp64 if a.mode == "fast" else None,
                          "ms_per_launch": [ms1, ms2],
                          "algorithmic_bytes_per_launch": [STAGE_BYTES[0] * cells, STAGE_BYTES[1] * cells]},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s",
