@@ -17,6 +17,8 @@
 #ifndef MBM_B200_H
 #define MBM_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -98,6 +100,13 @@ int mbm_create_batch(const mbm_block_desc *blocks, int nblocks, const mbm_case_d
 /* t[c], tend[c], nsteps[c], nrej[c] per case; max_steps > 0 caps accepted steps */
 int mbm_steps_batch(mbm_ctx *ctx, double *t, const double *tend, double CFLmax, double CFLreg,
                     int max_steps, int *nsteps, int *nrej);
+/* The same in two halves, no counterpart in the reference: _async launches the step
+ * loop of every case and returns; _wait waits for it and returns t, nsteps, nrej as
+ * above.  In between the host may do its own work (write the previous output) and
+ * call mbm_output_fields_async/mbm_output_wait; no other call on the context. */
+int mbm_steps_batch_async(mbm_ctx *ctx, const double *t, const double *tend, double CFLmax, double CFLreg,
+                          int max_steps);
+int mbm_steps_batch_wait(mbm_ctx *ctx, double *t, int *nsteps, int *nrej);
 
 /* Copy one block of a layer between the host (array of structs, (nx+6)*(ny+6)*9
  * doubles, the reference's CVector layer, src/defs.h:42-44) and the device. */
@@ -109,6 +118,18 @@ int mbm_download(mbm_ctx *ctx, int layer, int block, double *cells);
  * x outer, y inner, variables fastest; (nx+2)*(ny+2)*10 floats (single = 1) or
  * doubles, the bytes the reference writes to its .dat file. */
 int mbm_output_fields(mbm_ctx *ctx, int block, int single, void *out);
+
+/* The same payload formed now (from DATA as it is) into device memory the context
+ * keeps per block, and copied to `host` (page-locked, e.g. from mbm_host_alloc) on a
+ * stream of its own, so that the copy runs beside the next step loop; mbm_output_wait
+ * returns once every such copy has landed.  No counterpart in the reference, whose
+ * Output runs between intervals. */
+int mbm_output_fields_async(mbm_ctx *ctx, int block, int single, void *host);
+int mbm_output_wait(mbm_ctx *ctx);
+
+/* Page-locked host memory for mbm_output_fields_async (cudaMallocHost / cudaFreeHost). */
+int mbm_host_alloc(size_t bytes, void **p);
+int mbm_host_free(void *p);
 
 /* Dirichlet ghost values of one edge (code -2), in FillEdge's order: tangential
  * index over the full edge, corners included, outer; ghost layer n = 1..3 inner

@@ -99,29 +99,10 @@ def main(argv=None) -> int:
     device = int(_arg(argv, "-device", "0"))
     print("\n Running: Kn = %.4g, R13 = %g, CFL = %.2f, limiter = %s, BlockFile = \"%s\"" %
           (deck.Kn, deck.R13, deck.CFL, bf.limiter_name(deck.limiter), _arg(argv, "-bfile", "blockfile.txt")))
-    w = out.Writer(out_dir, deck, scn.type_name, single)
     sfile = _arg(argv, "-sfile")
+    initial = load_restart(deck, sfile, faithful="-restart-faithful" in argv) if sfile else None
     mode = "fast" if "-fast" in argv else "exact"
-    with sv.Solver(deck, scn, device=device, mode=mode) as s:
-        if sfile:
-            for b, U in enumerate(load_restart(deck, sfile, faithful="-restart-faithful" in argv)):
-                s.upload(sv.L_DATA, b, U)
-            s.set_boundary(sv.L_DATA, 0.0)
-        else:
-            s.initialise()
-        w.write_solver(s, 0.0, -1)
-        t, nmax = 0.0, 0
-        for tn in deck.t_out:
-            t0 = time.perf_counter()
-            t, n, rej = s.steps(t, tn, 1.0, deck.CFL)
-            el = time.perf_counter() - t0
-            for step, cfl, tt, dt in s.trace():
-                print(" step: %3d... done.  CFL: %lf, time: %lf, next dt: %lf" % (step, cfl, tt, dt))
-            print("   %d steps (%d rejected) to t = %g, %.4f us per cell-update" %
-                  (n, rej, t, el * 1e6 / max(1, deck.full_grid_size * (n + rej))))
-            nmax += n
-            w.write_solver(s, t, nmax)
-    print("\n Done after %d steps.\n" % nmax)
+    sv.run(deck, scn, out_dir, single=single, device=device, verbose=True, mode=mode, initial=initial)
     return 0
 
 

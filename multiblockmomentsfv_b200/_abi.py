@@ -27,7 +27,8 @@ EXPORTS = (
     "mbm_shard_plan", "mbm_create_sharded", "mbm_shard_buffers", "mbm_shard_set_dirichlet",
     "mbm_shard_begin", "mbm_shard_stage",
     "mbm_shard_pack", "mbm_shard_fill", "mbm_shard_cfl", "mbm_shard_control", "mbm_shard_end",
-    "mbm_fastmath_check",
+    "mbm_fastmath_check", "mbm_steps_batch_async", "mbm_steps_batch_wait", "mbm_output_fields_async",
+    "mbm_output_wait", "mbm_host_alloc", "mbm_host_free",
 )
 
 
@@ -98,6 +99,12 @@ def lib(path: str = None):
     L.mbm_shard_control.argtypes = [vp, ip]
     L.mbm_shard_end.argtypes = [vp, dp, ip, ip]
     L.mbm_fastmath_check.argtypes = [vp, C.c_int, vp]
+    L.mbm_steps_batch_async.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_int]
+    L.mbm_steps_batch_wait.argtypes = [vp, dp, ip, ip]
+    L.mbm_output_fields_async.argtypes = [vp, C.c_int, C.c_int, vp]
+    L.mbm_output_wait.argtypes = [vp]
+    L.mbm_host_alloc.argtypes = [C.c_size_t, P(vp)]
+    L.mbm_host_free.argtypes = [vp]
     L.mbm_config.argtypes = [vp, P(C.c_int), P(C.c_int), P(C.c_int)]
     L.mbm_create_batch.argtypes = [P(BlockDesc), C.c_int, P(CaseDesc), C.c_int, P(Params), P(vp)]
     L.mbm_steps_batch.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_int, P(C.c_int), P(C.c_int)]

@@ -103,6 +103,11 @@ struct mbm_ctx {
   cudaEvent_t ev = nullptr;
   // limiter groups of one stage run concurrently: forked from `stream`, joined back
   cudaStream_t aux[4] = {};
+  // output staged on the device and copied to the host beside the next interval
+  double* out_stage = nullptr;
+  std::vector<size_t> out_off;     // bytes, per block (room for the Float64 payload)
+  cudaStream_t out_stream = nullptr;
+  cudaEvent_t out_ev = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev[4] = {};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -767,6 +772,10 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   if (c->hcfl) cudaFreeHost(c->hcfl);
   if (c->ev) cudaEventDestroy(c->ev);
   if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+  if (c->out_stream) cudaStreamSynchronize(c->out_stream);
+  cudaFree(c->out_stage);
+  if (c->out_ev) cudaEventDestroy(c->out_ev);
+  if (c->out_stream) cudaStreamDestroy(c->out_stream);
   for (int k = 0; k < 4; k++) {
     if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
     if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
@@ -814,6 +823,51 @@ extern "C" int mbm_output_fields(mbm_ctx* c, int block, int single, void* out) {
                           single, c->staging, c->stream));
   CK(cudaMemcpyAsync(out, c->staging, bytes, cudaMemcpyDeviceToHost, c->stream));
   return wait_stream(c);
+}
+
+extern "C" int mbm_output_fields_async(mbm_ctx* c, int block, int single, void* host) {
+  if (!c || !host || block < 0 || block >= c->nblk) return fail(c, MBM_EINVAL, "mbm_output_fields_async: bad argument");
+  CK(cudaSetDevice(c->device));
+  if (!c->out_stage) {   // one payload area per block, an own stream for the copies
+    size_t off = 0;
+    for (auto& d : c->hblk) {
+      c->out_off.push_back(off);
+      off += ((size_t)(d.nxp - 4) * (d.nyp - 4) * 10 * sizeof(double) + 255) & ~(size_t)255;
+    }
+    CK(cudaMalloc(&c->out_stage, off));
+    CK(cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->out_ev, cudaEventDisableTiming));
+  }
+  const BlockDev& d = c->hblk[block];
+  const size_t bytes = (size_t)(d.nxp - 4) * (d.nyp - 4) * 10 * (single ? sizeof(float) : sizeof(double));
+  char* dst = (char*)c->out_stage + c->out_off[block];
+  CK(launch_output_fields(c->buf[phys_of(c, MBM_L_DATA, block)] + d.off, d.nxp, d.nyp, d.pitch, d.plane,
+                          single, dst, c->stream));
+  CK(cudaEventRecord(c->out_ev, c->stream));
+  CK(cudaStreamWaitEvent(c->out_stream, c->out_ev, 0));
+  CK(cudaMemcpyAsync(host, dst, bytes, cudaMemcpyDeviceToHost, c->out_stream));
+  return MBM_OK;
+}
+
+extern "C" int mbm_output_wait(mbm_ctx* c) {
+  if (!c) return fail(c, MBM_EINVAL, "mbm_output_wait: null context");
+  if (!c->out_stream) return MBM_OK;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->out_stream));
+  return MBM_OK;
+}
+
+extern "C" int mbm_host_alloc(size_t bytes, void** p) {
+  if (!p) return fail(nullptr, MBM_EINVAL, "mbm_host_alloc: null argument");
+  *p = nullptr;
+  const cudaError_t e = cudaMallocHost(p, bytes > 0 ? bytes : 1);
+  if (e != cudaSuccess) return fail(nullptr, e == cudaErrorMemoryAllocation ? MBM_ENOMEM : MBM_ECUDA, cudaGetErrorString(e));
+  return MBM_OK;
+}
+
+extern "C" int mbm_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+  return MBM_OK;
 }
 
 extern "C" int mbm_set_dirichlet(mbm_ctx* c, int block, int side, const double* values) {
@@ -891,10 +945,11 @@ extern "C" int mbm_time_update(mbm_ctx* c, double dt, double t, double* cfl) {
 
 // Steps for every case at once: each case has its own t, tend and dt; the loop
 // ends when every case is done (t >= tend, max_steps reached, or a failure).
-extern "C" int mbm_steps_batch(mbm_ctx* c, double* t, const double* tend, double CFLmax, double CFLreg,
-                               int max_steps, int* nsteps, int* nrej) {
-  if (c && c->sharded) return fail(c, MBM_EINVAL, "mbm_steps: the context holds part of a sharded case (mbm_shard_*)");
+// the step loop of every case, launched; mbm_steps_batch_wait collects it
+extern "C" int mbm_steps_batch_async(mbm_ctx* c, const double* t, const double* tend, double CFLmax,
+                                     double CFLreg, int max_steps) {
   if (!c || !t || !tend || max_steps < 0) return fail(c, MBM_EINVAL, "mbm_steps: bad argument");
+  if (c->sharded) return fail(c, MBM_EINVAL, "mbm_steps: the context holds part of a sharded case (mbm_shard_*)");
   CK(cudaSetDevice(c->device));
   bool any = false;
   for (int k = 0; k < c->ncase; k++) {
@@ -933,6 +988,13 @@ extern "C" int mbm_steps_batch(mbm_ctx* c, double* t, const double* tend, double
       if (!live) break;
     }
   }
+  return MBM_OK;
+}
+
+extern "C" int mbm_steps_batch_wait(mbm_ctx* c, double* t, int* nsteps, int* nrej) {
+  if (!c || !t) return fail(c, MBM_EINVAL, "mbm_steps: bad argument");
+  CK(cudaSetDevice(c->device));
+  int st;
   CK(cudaMemcpyAsync(c->hcase, c->dcase, sizeof(CaseDev) * c->ncase, cudaMemcpyDeviceToHost, c->stream));
   if ((st = wait_stream(c))) return st;
   int worst = 0;
@@ -946,6 +1008,13 @@ extern "C" int mbm_steps_batch(mbm_ctx* c, double* t, const double* tend, double
   if (worst == 2) return fail(c, MBM_ENONFINITE, "a stage wrote NaN or infinity, or CFL or dt became non-finite");
   if (worst == 5) return fail(c, MBM_ESTEPLIMIT, "step attempts exceeded max_attempts");
   return MBM_OK;
+}
+
+extern "C" int mbm_steps_batch(mbm_ctx* c, double* t, const double* tend, double CFLmax, double CFLreg,
+                               int max_steps, int* nsteps, int* nrej) {
+  int st = mbm_steps_batch_async(c, t, tend, CFLmax, CFLreg, max_steps);
+  if (st) return st;
+  return mbm_steps_batch_wait(c, t, nsteps, nrej);
 }
 
 extern "C" int mbm_steps_capped(mbm_ctx* c, double* t, double tend, double CFLmax, double CFLreg,

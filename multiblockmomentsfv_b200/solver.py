@@ -96,6 +96,15 @@ class Solver:
         self._check(self.L.mbm_output_fields(self.ctx, b, 1 if single else 0, a.ctypes.data))
         return a
 
+    def output_fields_async(self, b: int, out, single: bool = True) -> None:
+        """Start forming block b's payload and copying it to `out`, page-locked host
+        memory of ((nx+2)*(ny+2), 10) float32/float64 (see PinnedArray); the copy runs
+        beside the next step loop until output_wait()."""
+        self._check(self.L.mbm_output_fields_async(self.ctx, b, 1 if single else 0, out.ctypes.data))
+
+    def output_wait(self) -> None:
+        self._check(self.L.mbm_output_wait(self.ctx))
+
     def set_dirichlet(self, b: int, side: int, values: np.ndarray) -> None:
         v = np.ascontiguousarray(values, dtype=np.float64)
         self._check(self.L.mbm_set_dirichlet(self.ctx, b, side, _dptr(v)))
@@ -140,6 +149,20 @@ class Solver:
         self._check(self.L.mbm_steps_capped(self.ctx, C.byref(tt), tend, CFLmax, CFLreg, max_steps,
                                             C.byref(n), C.byref(r)))
         return tt.value, n.value, r.value
+
+    def steps_async(self, t: float, tend: float, CFLmax: float = 1.0, CFLreg: Optional[float] = None,
+                    max_steps: int = 0) -> None:
+        """Launch Steps() and return at once; steps_wait() collects (t, steps, rejections)."""
+        CFLreg = self.deck.CFL if CFLreg is None else CFLreg
+        tt = np.array([t], dtype=np.float64)
+        te = np.array([tend], dtype=np.float64)
+        self._check(self.L.mbm_steps_batch_async(self.ctx, _dptr(tt), _dptr(te), CFLmax, CFLreg, max_steps))
+
+    def steps_wait(self):
+        tt = np.zeros(1)
+        n, r = C.c_int(0), C.c_int(0)
+        self._check(self.L.mbm_steps_batch_wait(self.ctx, _dptr(tt), C.byref(n), C.byref(r)))
+        return float(tt[0]), n.value, r.value
 
     def attempts(self) -> int:
         a = C.c_int(0)
@@ -314,28 +337,79 @@ def ghost_map(blocks: Sequence[bf.Block]) -> np.ndarray:
     return arr[:n.value]
 
 
+class PinnedArray:
+    """A numpy array over page-locked host memory (mbm_host_alloc), for the
+    asynchronous output copies."""
+
+    def __init__(self, shape, dtype):
+        self.L = _abi.lib()
+        dt = np.dtype(dtype)
+        nbytes = int(np.prod(shape)) * dt.itemsize
+        p = C.c_void_p()
+        _abi.check(self.L.mbm_host_alloc(nbytes, C.byref(p)))
+        self._p = p
+        buf = (C.c_char * max(1, nbytes)).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)
+
+    def __del__(self):
+        try:
+            if self._p:
+                self.L.mbm_host_free(self._p)
+                self._p = None
+        except Exception:
+            pass
+
+
 def run(deck: bf.Deck, scenario: sc.Scenario, out_dir: str, single: bool = True, device: int = 0,
-        verbose: bool = True, show_every: int = 20, mode: str = "exact"):
+        verbose: bool = True, show_every: int = 20, mode: str = "exact", overlap: bool = True,
+        initial: Optional[Sequence[np.ndarray]] = None):
     """The reference's main() loop on the device: initial state and output at t=0,
-    then Steps + Output per output time (src/Main.c:138-156).  Returns (writer, steps)."""
+    then Steps + Output per output time (src/Main.c:138-156).  Returns (writer, steps).
+    overlap: each interval's output is formed on the device right after the interval,
+    copied to the host beside the next interval and written to the files while the
+    GPU steps on (same files as without).  initial: L_DATA layers to start from (a
+    restart) instead of the scenario's initial state."""
     w = out.Writer(out_dir, deck, scenario.type_name, single)
+    ft = np.float32 if single else np.float64
     with Solver(deck, scenario, device=device, show_every=show_every, mode=mode) as s:
-        s.initialise()
+        if initial is not None:
+            for b, U in enumerate(initial):
+                s.upload(L_DATA, b, U)
+            s.set_boundary(L_DATA, 0.0)
+        else:
+            s.initialise()
         w.write_solver(s, 0.0, -1)
         t, nmax = 0.0, 0
         cells = deck.full_grid_size
+        pins = [PinnedArray(((b.nx + 2) * (b.ny + 2), 10), ft) for b in deck.blocks] if overlap else None
+        pending = None                      # (t, step count) of an output staged but not written
         for tn in deck.t_out:
             t0 = time.perf_counter()
-            t, n, rej = s.steps(t, tn, 1.0, deck.CFL)
+            if overlap:
+                s.steps_async(t, tn, 1.0, deck.CFL)
+                if pending is not None:     # the previous output goes to disk while this interval runs
+                    s.output_wait()
+                    w._write([p.array.tobytes() for p in pins], *pending)
+                    pending = None
+                t, n, rej = s.steps_wait()
+            else:
+                t, n, rej = s.steps(t, tn, 1.0, deck.CFL)
             el = time.perf_counter() - t0
             if verbose:
                 for step, cfl, tt, dt in s.trace():
                     print(" step: %3d... done.  CFL: %lf, time: %lf, next dt: %lf" % (step, cfl, tt, dt))
                 perf = el * 1e6 / max(1, cells * (n + rej))
-                print("   %d steps (%d rejected) to t = %g in %.3f s, %.4f us per cell-update" %
-                      (n, rej, t, el, perf))
+                print("   %d steps (%d rejected) to t = %g, %.4f us per cell-update" % (n, rej, t, perf))
             nmax += n
-            w.write_solver(s, t, nmax)
+            if overlap:
+                for b in range(len(deck.blocks)):
+                    s.output_fields_async(b, pins[b].array, single)
+                pending = (t, nmax)
+            else:
+                w.write_solver(s, t, nmax)
+        if pending is not None:
+            s.output_wait()
+            w._write([p.array.tobytes() for p in pins], *pending)
     if verbose:
         print("\n Done after %d steps.\n" % nmax)
     return w, nmax
