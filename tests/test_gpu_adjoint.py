@@ -29,12 +29,12 @@ def _theta0(d, rng):
             * rng.uniform(0.5, 1.0) for b in d.blocks]
 
 
-def _fd_check(n, nsteps, every, ndirs, seed, limiter=bf.LIM_AVERAGE, eps=1e-6, Kn=0.01):
+def _fd_check(n, nsteps, every, ndirs, seed, limiter=bf.LIM_AVERAGE, eps=1e-6, Kn=0.01, mode="exact"):
     d = H.quadrant_deck(n, Kn=Kn, limiter=limiter)
     base = adj.smooth_base(d, seed)
     rng = np.random.default_rng(seed)
     th0 = _theta0(d, rng)
-    with adj.Sensitivity(d, base) as S:
+    with adj.Sensitivity(d, base, mode=mode) as S:
         layers = adj.state_from_theta(d, base, th0)
         S.load(layers)
         J, g, gK, dts, ms = S.run(nsteps, every)
@@ -63,6 +63,14 @@ def _fd_check(n, nsteps, every, ndirs, seed, limiter=bf.LIM_AVERAGE, eps=1e-6, K
 def test_adjoint_smooth_limiters(limiter):
     worst, errK, ms, J = _fd_check(n=24, nsteps=12, every=5, ndirs=6, seed=3, limiter=limiter)
     assert J > 0
+    assert worst < 1e-6, worst
+    assert errK < 1e-6, errK
+
+
+def test_adjoint_with_the_fast_forward():
+    """The same gradient checked against differences of the fast-arithmetic forward
+    map (the adjoint differentiates the mathematics both modes compute)."""
+    worst, errK, ms, J = _fd_check(n=24, nsteps=12, every=5, ndirs=6, seed=3, mode="fast")
     assert worst < 1e-6, worst
     assert errK < 1e-6, errK
 
