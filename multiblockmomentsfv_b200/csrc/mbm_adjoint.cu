@@ -322,6 +322,269 @@ __global__ void sum_partials(const double* part, int n, double* J) {
   }
 }
 
+// ------------------------------------------------------------------ row march --
+// The same stage adjoint in one pass, marching up a strip of rows like the forward
+// stage kernel.  One warp: lanes <-> columns C = I0-3 .. I0+28, outputs the 26 columns
+// I0 .. I0+25 (lanes 3..28) of the non-ring cells of a row segment [J0, J1).  Iteration
+// r brings row r: its projected primitives into a four-row window, the stage-output
+// adjoint of row r-1 into a three-row window; then the y face (r-2 | r-1) -- its HLL
+// adjoint, the slope adjoint of row r-2 and its limiter derivatives, scattered into the
+// per-row accumulators of rows r-3 .. r-1 -- and, with row r-3 complete in y, its x faces
+// (shuffles), the x slope terms, and the cell step (relaxation, Primitive, update term,
+// Data0) for the 26 output cells.  Each slope and limiter derivative is evaluated once,
+// nothing but the adjoint layers goes through global memory.  It is an independent second
+// implementation of the stage adjoint (MBM_ADJ_MARCH=1; tests require both to agree);
+// its 23 KB of shared memory per warp leave 8 warps per SM, too few to hide its
+// dependency chains, and it runs 25 % slower than the three-pass version, the default.
+struct AdjWindow {
+  double P[4][NV][32];      // projected primitives, rows r-3 .. r
+  double L[3][NV][32];      // stage-output adjoint (zero off the interior), rows r-3 .. r-1
+  double A[3][NV][32];      // y-direction accumulators of the primitive adjoint, rows r-3 .. r-1
+};
+constexpr int AWARPS = 4;
+
+__device__ __forceinline__ int s3(int q) { return (q + 6) % 3; }
+__device__ __forceinline__ int s4(int q) { return (q + 8) & 3; }
+
+__device__ __forceinline__ void benign9(double* U) {
+  U[0] = 1.0; U[1] = 0.0; U[2] = 0.0; U[3] = 1.5; U[4] = 1.0;
+  U[5] = 0.0; U[6] = 1.0; U[7] = 0.0; U[8] = 0.0;
+}
+
+template <int HEUN, int LIM>
+__device__ __forceinline__ double march_item(const AdjArgs& a, const Work w, const int lane, AdjWindow& win) {
+  const BlockDev B = a.blk[w.blk];
+  const int nxp = B.nxp, nyp = B.nyp;
+  const long long pitch = B.pitch, plane = B.plane;
+  const double* __restrict__ x = a.x + B.off;
+  const double* __restrict__ lout = a.lout + B.off;
+  const int C = w.I0 - 3 + lane;
+  const bool col_in = C >= 0 && C < nxp;
+  const bool col_ring = C == 0 || C == nxp - 1;
+  const bool col_inner = C >= NG && C <= nxp - 1 - NG;
+  const bool out_lane = lane >= 3 && lane <= 28 && C <= nxp - 2;
+  const double rdx = mbm_adj::rcp(B.dx), rdy = mbm_adj::rcp(B.dy);
+  const double hdx = 0.5 * B.dx, hdy = 0.5 * B.dy;
+  const double s = HEUN ? 0.5 : 1.0;
+  const double cx = s * a.dt * rdx, cy = s * a.dt * rdy;
+  const int rs = w.J0 - 3;
+  double knb = 0.0;
+  double grp[NV];                     // right-state adjoint of the previous y face
+#pragma unroll
+  for (int m = 0; m < NV; m++) grp[m] = 0.0;
+  for (int r = rs; r <= w.J1 + 2; r++) {
+    // (A) row r: projected primitives; stage-output adjoint of row r-1
+    {
+      double U[NV], P[NV];
+      const bool ok = col_in && r >= 0 && r < nyp;
+      if (ok) {
+#pragma unroll
+        for (int m = 0; m < NV; m++) U[m] = x[m * plane + (long long)r * pitch + C + 1];
+      } else {
+        benign9(U);
+      }
+      mbm_adj::prim(U, P);
+      if (ok && !(col_ring || r == 0 || r == nyp - 1)) {
+        double Q[NV];
+        mbm_adj::relax_p(P, Q, a.dt, a.Kn, a.F, 2 * HEUN + 1);
+#pragma unroll
+        for (int m = 0; m < NV; m++) P[m] = Q[m];
+      }
+#pragma unroll
+      for (int m = 0; m < NV; m++) win.P[s4(r)][m][lane] = P[m];
+      const int q = r - 1;
+      const bool lin = col_inner && q >= NG && q <= nyp - 1 - NG;
+#pragma unroll
+      for (int m = 0; m < NV; m++)
+        win.L[s3(q)][m][lane] = lin ? lout[m * plane + (long long)q * pitch + C + 1] : 0.0;
+    }
+    // (B) y face (q | q+1), q = r-2: HLL adjoint, slope adjoint of row q
+    if (r >= rs + 3) {
+      const int q = r - 2;
+#pragma unroll
+      for (int m = 0; m < NV; m++) win.A[s3(r - 1)][m][lane] = 0.0;   // row r-1: first contribution now
+      double fb[NV];
+      bool any = false;
+#pragma unroll
+      for (int m = 0; m < NV; m++) {
+        fb[m] = cy * (win.L[s3(q + 1)][m][lane] - win.L[s3(q)][m][lane]);
+        any = any || fb[m] != 0.0;
+      }
+      any = any && out_lane;
+      double gl[NV] = {0}, gr[NV] = {0};
+      if (any) {
+        double PL[NV], PR[NV];
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          const double pm = win.P[s4(q - 1)][m][lane], p0 = win.P[s4(q)][m][lane];
+          const double p1 = win.P[s4(q + 1)][m][lane], p2 = win.P[s4(q + 2)][m][lane];
+          PL[m] = p0 + hdy * (mbm_adj::limit_val(LIM, p0 - pm, p1 - p0) * rdy);
+          PR[m] = p1 - hdy * (mbm_adj::limit_val(LIM, p1 - p0, p2 - p1) * rdy);
+        }
+        mbm_adj::hll_p_adj(PL, PR, fb, gl, gr, 2);
+      }
+      if (out_lane) {
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          double acc = win.A[s3(q)][m][lane] + gl[m] + grp[m];          // direct terms of row q
+          const double ls = hdy * (gl[m] - grp[m]);                     // adjoint of S_y(q)
+          if (ls != 0.0) {
+            const double pm = win.P[s4(q - 1)][m][lane], p0 = win.P[s4(q)][m][lane];
+            const double p1 = win.P[s4(q + 1)][m][lane];
+            double g1, g2;
+            mbm_adj::limit_grad(LIM, p0 - pm, p1 - p0, &g1, &g2);
+            win.A[s3(q - 1)][m][lane] -= ls * g1 * rdy;
+            acc += ls * (g1 - g2) * rdy;
+            win.A[s3(q + 1)][m][lane] += ls * g2 * rdy;
+          }
+          win.A[s3(q)][m][lane] = acc;
+          grp[m] = gr[m];
+        }
+      }
+    }
+    // (C) row c = r-3, complete in y: x faces, x slope terms, the cell step
+    if (r >= rs + 6) {
+      const int c = r - 3;
+      const bool xface = lane >= 1 && lane <= 29;
+      double P0[NV], PL[NV], PR[NV], fbx[NV], glx[NV] = {0}, grx[NV] = {0};
+      bool anyx = false;
+#pragma unroll
+      for (int m = 0; m < NV; m++) {
+        const double p = win.P[s4(c)][m][lane];
+        const double pm = __shfl_up_sync(0xffffffffu, p, 1);
+        const double pp = __shfl_down_sync(0xffffffffu, p, 1);
+        const double pp2 = __shfl_down_sync(0xffffffffu, p, 2);
+        const double lam = win.L[s3(c)][m][lane];
+        const double lamr = __shfl_down_sync(0xffffffffu, lam, 1);
+        P0[m] = p;
+        fbx[m] = xface ? cx * (lamr - lam) : 0.0;
+        anyx = anyx || fbx[m] != 0.0;
+        PL[m] = p + hdx * (mbm_adj::limit_val(LIM, p - pm, pp - p) * rdx);
+        PR[m] = pp - hdx * (mbm_adj::limit_val(LIM, pp - p, pp2 - pp) * rdx);
+      }
+      if (anyx) mbm_adj::hll_p_adj(PL, PR, fbx, glx, grx, 1);
+      double Pb[NV];
+#pragma unroll
+      for (int m = 0; m < NV; m++) {
+        const double p = P0[m];
+        const double pm = __shfl_up_sync(0xffffffffu, p, 1);
+        const double pp = __shfl_down_sync(0xffffffffu, p, 1);
+        double grm = __shfl_up_sync(0xffffffffu, grx[m], 1);
+        if (lane == 0) grm = 0.0;
+        const double ls = hdx * (glx[m] - grm);                          // adjoint of S_x(lane)
+        double ga = 0.0, gb = 0.0;
+        if (ls != 0.0) {
+          double g1, g2;
+          mbm_adj::limit_grad(LIM, p - pm, pp - p, &g1, &g2);
+          ga = ls * g1 * rdx;
+          gb = ls * g2 * rdx;
+        }
+        double bl = __shfl_up_sync(0xffffffffu, gb, 1);
+        double ar = __shfl_down_sync(0xffffffffu, ga, 1);
+        if (lane == 0) bl = 0.0;
+        if (lane == 31) ar = 0.0;
+        Pb[m] = (out_lane ? win.A[s3(c)][m][lane] : 0.0) + glx[m] + grm + (ga - gb) + bl - ar;
+      }
+      if (out_lane) {
+        const long long ic = (long long)c * pitch + C + 1;
+        double U[NV], Pr[NV], Qb[NV] = {0}, Ub[NV] = {0}, Vb[NV] = {0};
+#pragma unroll
+        for (int m = 0; m < NV; m++) U[m] = x[m * plane + ic];
+        mbm_adj::prim(U, Pr);
+        bool anyP = false;
+#pragma unroll
+        for (int m = 0; m < NV; m++) anyP = anyP || Pb[m] != 0.0;
+        if (anyP) mbm_adj::relax_p_adj(Pr, Pb, Qb, &knb, a.dt, a.Kn, 2 * HEUN + 1);
+        if (col_inner && c >= NG && c <= nyp - 1 - NG) {
+          double Rb[NV], Q[NV], Cb[NV] = {0};
+#pragma unroll
+          for (int m = 0; m < NV; m++) Rb[m] = s * win.L[s3(c)][m][lane];
+          mbm_adj::relax_p(Pr, Q, a.dt, a.Kn, a.F, 2 * HEUN);
+          mbm_adj::cons_adj(Q, Rb, Cb);
+          mbm_adj::relax_p_adj(Pr, Cb, Qb, &knb, a.dt, a.Kn, 2 * HEUN);
+          if (HEUN) {
+            double V[NV], W[NV], Q2[NV], C2[NV] = {0}, Pd[NV] = {0};
+#pragma unroll
+            for (int m = 0; m < NV; m++) V[m] = a.d0[B.off + m * plane + ic];
+            mbm_adj::prim(V, W);
+            mbm_adj::relax_p(W, Q2, a.dt, a.Kn, a.F, -1);
+            mbm_adj::cons_adj(Q2, Rb, C2);
+            mbm_adj::relax_p_adj(W, C2, Pd, &knb, a.dt, a.Kn, -1);
+            mbm_adj::prim_adj(V, Pd, Vb);
+          }
+        }
+        bool anyQ = false;
+#pragma unroll
+        for (int m = 0; m < NV; m++) anyQ = anyQ || Qb[m] != 0.0;
+        if (anyQ) mbm_adj::prim_adj(U, Qb, Ub);
+        if (HEUN) {           // stage 2 starts both adjoint layers (their ring is cleared beforehand)
+#pragma unroll
+          for (int m = 0; m < NV; m++) {
+            a.lx[B.off + m * plane + ic] = Ub[m];
+            a.ld0[B.off + m * plane + ic] = Vb[m];
+          }
+        } else if (anyQ) {
+#pragma unroll
+          for (int m = 0; m < NV; m++) a.lx[B.off + m * plane + ic] += Ub[m];
+        }
+      }
+    }
+  }
+  return knb;
+}
+
+template <int HEUN, int LIM>
+__global__ void __launch_bounds__(32 * AWARPS, 2) adj_march(AdjArgs a) {
+  extern __shared__ __align__(16) unsigned char adj_smem[];
+  AdjWindow* win = reinterpret_cast<AdjWindow*>(adj_smem);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double knb = 0.0;
+  for (;;) {
+    int w = 0;
+    if (lane == 0) w = atomicAdd(a.queue, 1);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (w >= a.nwork) break;
+    knb += march_item<HEUN, LIM>(a, a.work[w], lane, win[warp]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) knb += __shfl_xor_sync(0xffffffffu, knb, o);
+  if (lane == 0 && knb != 0.0) atomicAdd(a.knb, knb);
+}
+
+constexpr int ADJ_SMEM = (int)sizeof(AdjWindow) * AWARPS;
+
+template <int HEUN, int LIM>
+static void march_attr() {
+  cudaFuncSetAttribute(adj_march<HEUN, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, ADJ_SMEM);
+}
+
+// CTAs per SM of the row-marching pass (allows its dynamic shared memory first)
+int adjoint_march_ctas() {
+  march_attr<0, 0>(); march_attr<0, 1>(); march_attr<0, 2>(); march_attr<0, 3>(); march_attr<0, 4>();
+  march_attr<1, 0>(); march_attr<1, 1>(); march_attr<1, 2>(); march_attr<1, 3>(); march_attr<1, 4>();
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adj_march<1, 4>, 32 * AWARPS, ADJ_SMEM);
+  return n > 0 ? n : 1;
+}
+
+template <int HEUN>
+static void march_lim(const AdjArgs& a, int grid, cudaStream_t s) {
+  switch (a.limiter) {
+    case 0: adj_march<HEUN, 0><<<grid, 32 * AWARPS, ADJ_SMEM, s>>>(a); break;
+    case 1: adj_march<HEUN, 1><<<grid, 32 * AWARPS, ADJ_SMEM, s>>>(a); break;
+    case 2: adj_march<HEUN, 2><<<grid, 32 * AWARPS, ADJ_SMEM, s>>>(a); break;
+    case 3: adj_march<HEUN, 3><<<grid, 32 * AWARPS, ADJ_SMEM, s>>>(a); break;
+    default: adj_march<HEUN, 4><<<grid, 32 * AWARPS, ADJ_SMEM, s>>>(a); break;
+  }
+}
+
+// one stage's adjoint by the row-marching pass; a.queue must be zero
+cudaError_t adjoint_stage_march(const AdjArgs& a, int grid, cudaStream_t s) {
+  if (a.heun) march_lim<1>(a, grid, s);
+  else march_lim<0>(a, grid, s);
+  return cudaGetLastError();
+}
+
 cudaError_t adjoint_stage(const AdjArgs& a0, long long nthr, double* FLx, double* FRx, double* FLy,
                           double* FRy, cudaStream_t s) {
   const int T = 128;

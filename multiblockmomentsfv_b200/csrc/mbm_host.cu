@@ -45,6 +45,8 @@ cudaError_t launch_ckpt(const CaseDev* cases, const double* buf0, const double* 
 cudaError_t adjoint_stage(const AdjArgs& a0, long long ncell, double* FLx, double* FRx, double* FLy,
                           double* FRy, cudaStream_t s);
 cudaError_t adjoint_ghosts(const BlockDev* blk, const GhostEntry* map, int n, double* l, cudaStream_t s);
+cudaError_t adjoint_stage_march(const AdjArgs& a, int grid, cudaStream_t s);
+int adjoint_march_ctas();
 cudaError_t adjoint_functional(const BlockDev* blk, int nblk, const double* x, double* l, long long ncell,
                                double* part, double* J, cudaStream_t s);
 cudaError_t launch_fill_uniform(double* base, long long plane, cudaStream_t s);
@@ -132,6 +134,11 @@ struct mbm_ctx {
   double* adj_scal = nullptr;       // [0] dJ/dKn, [1] J
   double* adj_dtrep = nullptr;      // dt values of mbm_replay
   double* adj_part = nullptr;       // per-CTA partial sums of J
+  // the row-marching adjoint pass (MBM_ADJ_MARCH=1; the three-pass one is the default)
+  bool adj_march = false;
+  Work* adj_work = nullptr;
+  int adj_nwork = 0, adj_grid = 0;
+  int* adj_queue = nullptr;
   int adj_nsteps = 0, adj_every = 0, adj_nrep = 0;
   std::string err;
 };
@@ -762,6 +769,8 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   cudaFree(c->adj_dtlog);
   cudaFree(c->adj_dtrep);
   cudaFree(c->adj_part);
+  cudaFree(c->adj_work);
+  cudaFree(c->adj_queue);
   cudaFree(c->adj_scal);
   cudaFree(c->dsend_list);
   cudaFree(c->shard_send);
@@ -1125,6 +1134,26 @@ static int adj_alloc(mbm_ctx* c, int nsteps, int every) {
     for (int k = 0; k < 8; k++) CK(cudaMalloc(&c->adj_buf[k], sizeof(double) * c->layer_elems));
   if (!c->adj_scal) CK(cudaMalloc(&c->adj_scal, sizeof(double) * 2));
   if (!c->adj_part) CK(cudaMalloc(&c->adj_part, sizeof(double) * ((adj_threads(c) + 127) / 128)));
+  if (!c->adj_work) {   // row-marching work: strips of ASTRIP columns x 32-row segments of the non-ring cells
+    const char* env = getenv("MBM_ADJ_MARCH");
+    c->adj_march = env && atoi(env) == 1;
+    std::vector<Work> wl;
+    for (int b = 0; b < c->nblk; b++) {
+      const BlockDev& d = c->hblk[b];
+      const int rows = d.nyp - 2, segs = (rows + 31) / 32;
+      for (int sg = 0; sg < segs; sg++) {
+        const int J0 = 1 + (int)((long long)rows * sg / segs), J1 = 1 + (int)((long long)rows * (sg + 1) / segs);
+        for (int I0 = 1; I0 <= d.nxp - 2; I0 += ASTRIP) wl.push_back(Work{b, I0, J0, J1});
+      }
+    }
+    c->adj_nwork = (int)wl.size();
+    CK(cudaMalloc(&c->adj_work, sizeof(Work) * std::max<size_t>(1, wl.size())));
+    CK(cudaMemcpyAsync(c->adj_work, wl.data(), sizeof(Work) * wl.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMalloc(&c->adj_queue, sizeof(int)));
+    c->adj_grid = std::max(1, std::min((c->adj_nwork + 3) / 4, c->nsm * adjoint_march_ctas()));
+    int st = wait_stream(c);
+    if (st) return st;
+  }
   if (nsteps > c->adj_nsteps || every != c->adj_every) {
     cudaFree(c->adj_ckpt);
     cudaFree(c->adj_seg);
@@ -1174,8 +1203,16 @@ static int adj_step(mbm_ctx* c, const double* Dn, const double* Tn, double dt, d
   double* P = c->adj_buf[3];
   const long long nc = adj_threads(c);
   const CaseDev& h = c->hcase[0];
-  // no clearing: stage 2's cell pass writes every cell of lamT and lam_next
+  // the three-pass cell pass writes every cell of lamT and lam_next in stage 2; the
+  // row-marching pass writes the non-ring cells, so the ring starts at zero
+  if (c->adj_march) {
+    CK(cudaMemsetAsync(lamT, 0, sizeof(double) * c->layer_elems, c->stream));
+    CK(cudaMemsetAsync(lam_next, 0, sizeof(double) * c->layer_elems, c->stream));
+  }
   AdjArgs a{};
+  a.work = c->adj_work;
+  a.nwork = c->adj_nwork;
+  a.queue = c->adj_queue;
   a.blk = c->dblk;
   a.nblk = c->nblk;
   a.P = P;
@@ -1191,7 +1228,12 @@ static int adj_step(mbm_ctx* c, const double* Dn, const double* Tn, double dt, d
   a.lout = lam;
   a.lx = lamT;
   a.ld0 = lam_next;
-  CK(adjoint_stage(a, nc, c->adj_buf[4], c->adj_buf[5], c->adj_buf[6], c->adj_buf[7], c->stream));
+  if (c->adj_march) {
+    CK(cudaMemsetAsync(c->adj_queue, 0, sizeof(int), c->stream));
+    CK(adjoint_stage_march(a, c->adj_grid, c->stream));
+  } else {
+    CK(adjoint_stage(a, nc, c->adj_buf[4], c->adj_buf[5], c->adj_buf[6], c->adj_buf[7], c->stream));
+  }
   CK(adjoint_ghosts(c->dblk, c->dghost, c->nghost, lamT, c->stream));
   // stage 1: TMP = stage1(D_n)
   a.heun = 0;
@@ -1200,7 +1242,12 @@ static int adj_step(mbm_ctx* c, const double* Dn, const double* Tn, double dt, d
   a.lout = lamT;
   a.lx = lam_next;
   a.ld0 = nullptr;
-  CK(adjoint_stage(a, nc, c->adj_buf[4], c->adj_buf[5], c->adj_buf[6], c->adj_buf[7], c->stream));
+  if (c->adj_march) {
+    CK(cudaMemsetAsync(c->adj_queue, 0, sizeof(int), c->stream));
+    CK(adjoint_stage_march(a, c->adj_grid, c->stream));
+  } else {
+    CK(adjoint_stage(a, nc, c->adj_buf[4], c->adj_buf[5], c->adj_buf[6], c->adj_buf[7], c->stream));
+  }
   CK(adjoint_ghosts(c->dblk, c->dghost, c->nghost, lam_next, c->stream));
   return MBM_OK;
 }

@@ -84,7 +84,12 @@ struct AdjArgs {       // one stage of the discrete adjoint (mbm_adjoint.cu)
   double* knb;           // += dJ/dKn
   double dt, Kn, F;
   int limiter, heun;
+  const Work* work;      // row-marching pass: strips of ASTRIP columns x row segments
+  int nwork;
+  int* queue;            // its work-item counter (zero before the launch)
 };
+
+constexpr int ASTRIP = 26;   // output columns of one warp of the row-marching adjoint
 
 __host__ __device__ inline int phys_layer(int sel, int cur) {
   return sel == SEL_CUR ? cur : (sel == SEL_OTHER ? 1 - cur : 2);

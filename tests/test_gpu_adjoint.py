@@ -165,3 +165,30 @@ def test_autograd_function():
         ref = np.stack(adj.theta_gradient(d, layers, g))
         assert np.allclose(th.grad.numpy(), ref, rtol=1e-12, atol=0)
         assert abs(float(kn.grad) - gK) <= 1e-12 * abs(gK)
+
+
+@pytest.mark.parametrize("limiter", [bf.LIM_NONE, bf.LIM_MINMOD, bf.LIM_SUPERBEE, bf.LIM_HARMONIC])
+def test_row_march_equals_three_pass(limiter):
+    """The row-marching adjoint pass (MBM_ADJ_MARCH=1) and the three-pass one (the
+    default), two independent implementations of the stage adjoint, give the same
+    gradient up to rounding (different association of the same sums)."""
+    import os
+    d = H.quadrant_deck(40, Kn=0.01, limiter=limiter)
+    base = adj.smooth_base(d, 13)
+    th0 = _theta0(d, np.random.default_rng(13))
+    out = {}
+    for march in ("1", "0"):
+        os.environ["MBM_ADJ_MARCH"] = march
+        try:
+            with adj.Sensitivity(d, base) as S:
+                layers = adj.state_from_theta(d, base, th0)
+                S.load(layers)
+                J, g, gK, dts, ms = S.run(16, 5)
+                out[march] = (J, np.concatenate([x.ravel() for x in g]), gK)
+        finally:
+            del os.environ["MBM_ADJ_MARCH"]
+    (J1, g1, k1), (J0, g0, k0) = out["1"], out["0"]
+    assert J1 == J0
+    scale = np.abs(g0).max()
+    assert np.abs(g1 - g0).max() <= 1e-11 * scale, np.abs(g1 - g0).max() / scale
+    assert abs(k1 - k0) <= 1e-11 * abs(k0)
