@@ -73,14 +73,17 @@ __device__ __forceinline__ double mk_div(double x, double y, double r) {
 __device__ __noinline__ double div_ieee(double x, double y) { return x / y; }
 
 // Reciprocal, square root and lone quotients.  Bitwise: IEEE division and sqrt.
-// Fast arithmetic: the Newton-refined hardware approximations of mbm_newton.cuh.
+// Fast arithmetic: the refined hardware approximations of mbm_newton.cuh (fsqrt1,
+// without the root's last correction, for wave speeds and collision frequencies).
 #if MBM_FAST_ARITH
 using mbm_newton::frcp;
 using mbm_newton::fsqrt;
+using mbm_newton::fsqrt1;
 __device__ __forceinline__ double fdiv(double x, double y) { return x * frcp(y); }
 #else
 __device__ __forceinline__ double fdiv(double x, double y) { return x / y; }
 __device__ __forceinline__ double fsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ double fsqrt1(double x) { return sqrt(x); }
 #endif
 
 struct Recip {        // 1/y for a denominator shared by several quotients
@@ -294,7 +297,7 @@ __device__ __forceinline__ double relax(const double (&P)[NV], double (&Out)[NV]
   double vs = v1 * v1 + v2 * v2;
   double E = 0.5 * rho * vs + 1.5 * rho * th;
   const double nu0 = 1.0;
-  const double num = nu0 * rho * fsqrt(th);
+  const double num = nu0 * rho * fsqrt1(th);
   const double coll = (__builtin_expect(mk_in(num), 1) ? Kn.exact(num) : div_ieee(num, Kn.y)) * dt;
   if (FLAG == 0 || FLAG == 2) {
     const double g0 = F, g1 = 0.0;
@@ -320,7 +323,7 @@ template <int FLAG>
 __device__ __forceinline__ void relax_prim(const double (&P)[NV], double (&Q)[NV], double dt,
                                            const Recip& Kn, double F) {
   const double rho = P[0], th = P[3];
-  const double coll = rho * fsqrt(th) * Kn.r * dt;
+  const double coll = rho * fsqrt1(th) * Kn.r * dt;
   const double d1 = rdamp<FLAG>(coll);
   const double d2 = rdamp<FLAG>(2.0 / 3 * coll);
   Q[0] = rho;
@@ -339,7 +342,7 @@ __device__ __forceinline__ void relax_prim(const double (&P)[NV], double (&Q)[NV
 template <int FLAG>
 __device__ __forceinline__ double relax_cfl(const double (&P)[NV], double dt, const Recip& Kn) {
   const double nu0 = 1.0;
-  const double num = nu0 * P[0] * fsqrt(P[3]);
+  const double num = nu0 * P[0] * fsqrt1(P[3]);
   const double coll = (__builtin_expect(mk_in(num), 1) ? Kn.exact(num) : div_ieee(num, Kn.y)) * dt;
   return 0.5 * (1 - rdamp<FLAG>(2.0 / 3 * coll));
 }
@@ -365,11 +368,49 @@ __device__ __forceinline__ double limit(double d1, double d2) {
 }
 
 #if MBM_FAST_ARITH
+// Conservative(P) and the Grad-13 flux along x of the same state (src/Flux.c:61-119
+// in primitive variables; fast arithmetic).  The flux's first four components are
+// moments (F0..F3 = U1, U4, U5, U7) and the others are regrouped around them:
+//   F4 = U1 (3 T11 + u^2) + 6/5 q1
+//   F5 = v U4 + 2 u rho T12 + 2/5 q2,   F6 = u U6 + 2 v rho T12 + 2/5 q1
+//   F7 = u (2 U7 - E u + 6/5 q1) + 2/5 q2 v + rho/2 (T11 (|v|^2 + 7 theta) - 2 theta^2)
+//   F8 = 7/5 (q2 u + q1 v) + u v (rho (T11 + T22) + E) + rho T12 (3/2 |v|^2 + 7/2 theta)
+// (E = U3; M111 = 6/5 q1/rho, M112 = M121 = 2/5 q2/rho, M122 = M221 = 2/5 q1/rho).
+__device__ __forceinline__ void cons_flux_x(const double (&P)[NV], double (&U)[NV], double (&F)[NV]) {
+  const double r = P[0], u = P[1], v = P[2], th = P[3];
+  const double T11 = P[4], T12 = P[5], T22 = P[6], q1 = P[7], q2 = P[8];
+  const double vs = u * u + v * v;
+  const double E = 0.5 * r * vs + 1.5 * r * th;
+  U[0] = r;
+  U[1] = r * u;
+  U[2] = r * v;
+  U[3] = E;
+  U[4] = r * (T11 + u * u);
+  U[5] = r * (T12 + u * v);
+  U[6] = r * (T22 + v * v);
+  U[7] = q1 + E * u + r * (T11 * u + T12 * v);
+  U[8] = q2 + E * v + r * (T12 * u + T22 * v);
+  const double q1a = 1.2 * q1, q1b = 0.4 * q1, q2b = 0.4 * q2;
+  const double rT12 = r * T12, t2 = rT12 + rT12;
+  F[0] = U[1];
+  F[1] = U[4];
+  F[2] = U[5];
+  F[3] = U[7];
+  F[4] = fma(U[1], fma(3.0, T11, u * u), q1a);
+  F[5] = fma(v, U[4], fma(u, t2, q2b));
+  F[6] = fma(u, U[6], fma(v, t2, q1b));
+  F[7] = fma(u, fma(-E, u, 2.0 * U[7]) + q1a,
+             fma(q2b, v, 0.5 * r * fma(T11, vs + 7.0 * th, -2.0 * th * th)));
+  F[8] = fma(1.4, fma(q2, u, q1 * v), fma(u * v, fma(r, T11 + T22, E), rT12 * fma(1.5, vs, 3.5 * th)));
+}
+
 // FnumHLLE (src/Flux.c:308-379) in primitive form (fast arithmetic): the Grad-13
 // flux straight from the face states -- no Conservative -> Primitive round trip and
 // no rotations (a y face swaps the x and y components, which is what the rotation
-// to the normal (0,1) amounts to); one reciprocal of alpha.  Mathematically the
-// bitwise version below; the rounding differs.
+// to the normal (0,1) amounts to); c = 2 sqrt(5/3 theta) as sqrt(20/3 theta); the
+// combination (lamR fL - lamL fR + lamL lamR (UR - UL)) / alpha with its three
+// coefficients formed once.  Mathematically the bitwise version below; the rounding
+// differs.
 template <int DIR>
 __device__ __forceinline__ double hll(const double (&PL_)[NV], const double (&PR_)[NV],
                                       double (&flx)[NV]) {
@@ -381,12 +422,10 @@ __device__ __forceinline__ double hll(const double (&PL_)[NV], const double (&PR
 #pragma unroll
     for (int n = 0; n < NV; n++) { PL[n] = PL_[n]; PR[n] = PR_[n]; }
   }
-  const double cR = 2.0 * fsqrt(5.0 / 3 * PR[3]);
-  const double cL = 2.0 * fsqrt(5.0 / 3 * PL[3]);
-  mbm_adj::cons(PL, UL);
-  mbm_adj::cons(PR, UR);
-  mbm_adj::gflux_x(PL, fL);
-  mbm_adj::gflux_x(PR, fR);
+  const double cR = fsqrt1(20.0 / 3 * PR[3]);
+  const double cL = fsqrt1(20.0 / 3 * PL[3]);
+  cons_flux_x(PL, UL, fL);
+  cons_flux_x(PR, UR, fR);
   const double vR = PR[1], vL = PL[1];
   const double cMax = fabs(0.5 * (vL + vR)) + rmax(cR, cL);
   const double lamL = rmin(vL - cL, 0.0);
@@ -395,8 +434,9 @@ __device__ __forceinline__ double hll(const double (&PL_)[NV], const double (&PR
   double f[NV];
   if (alph > 0.0) {
     const double ra = frcp(alph);
+    const double ca = lamR * ra, cb = lamL * ra, cc = lamL * ca;
 #pragma unroll
-    for (int n = 0; n < NV; n++) f[n] = (lamR * fL[n] - lamL * fR[n] + lamL * lamR * (UR[n] - UL[n])) * ra;
+    for (int n = 0; n < NV; n++) f[n] = fma(cc, UR[n] - UL[n], fma(-cb, fR[n], ca * fL[n]));
   } else {
 #pragma unroll
     for (int n = 0; n < NV; n++) f[n] = 0.5 * (fL[n] + fR[n]);
