@@ -186,9 +186,9 @@ int mbm_attempts(mbm_ctx *ctx, int *attempts);
 int mbm_case_status(mbm_ctx *ctx, int *status, int n);
 
 /* Diagnostic, no counterpart in the reference: the fast-arithmetic reciprocal and
- * square roots (MBM_MODE_FAST) of n values in device memory x; out (device, 3n
- * doubles) receives per x the reciprocal, the corrected root and the uncorrected
- * root, for comparison with correctly rounded results.  Normal positive operands. */
+ * square root (MBM_MODE_FAST) of n values in device memory x; out (device, 2n
+ * doubles) receives 1/x and sqrt(x) interleaved, for comparison with correctly
+ * rounded results.  Normal positive operands. */
 int mbm_fastmath_check(const double *x, int n, double *out);
 
 /* ---- One case split over ranks by block (one process per GPU) ----------------

@@ -73,17 +73,14 @@ __device__ __forceinline__ double mk_div(double x, double y, double r) {
 __device__ __noinline__ double div_ieee(double x, double y) { return x / y; }
 
 // Reciprocal, square root and lone quotients.  Bitwise: IEEE division and sqrt.
-// Fast arithmetic: the refined hardware approximations of mbm_newton.cuh (fsqrt1,
-// without the root's last correction, for wave speeds and collision frequencies).
+// Fast arithmetic: the refined hardware approximations of mbm_newton.cuh.
 #if MBM_FAST_ARITH
 using mbm_newton::frcp;
 using mbm_newton::fsqrt;
-using mbm_newton::fsqrt1;
 __device__ __forceinline__ double fdiv(double x, double y) { return x * frcp(y); }
 #else
 __device__ __forceinline__ double fdiv(double x, double y) { return x / y; }
 __device__ __forceinline__ double fsqrt(double x) { return sqrt(x); }
-__device__ __forceinline__ double fsqrt1(double x) { return sqrt(x); }
 #endif
 
 struct Recip {        // 1/y for a denominator shared by several quotients
@@ -297,7 +294,7 @@ __device__ __forceinline__ double relax(const double (&P)[NV], double (&Out)[NV]
   double vs = v1 * v1 + v2 * v2;
   double E = 0.5 * rho * vs + 1.5 * rho * th;
   const double nu0 = 1.0;
-  const double num = nu0 * rho * fsqrt1(th);
+  const double num = nu0 * rho * fsqrt(th);
   const double coll = (__builtin_expect(mk_in(num), 1) ? Kn.exact(num) : div_ieee(num, Kn.y)) * dt;
   if (FLAG == 0 || FLAG == 2) {
     const double g0 = F, g1 = 0.0;
@@ -323,7 +320,7 @@ template <int FLAG>
 __device__ __forceinline__ void relax_prim(const double (&P)[NV], double (&Q)[NV], double dt,
                                            const Recip& Kn, double F) {
   const double rho = P[0], th = P[3];
-  const double coll = rho * fsqrt1(th) * Kn.r * dt;
+  const double coll = rho * fsqrt(th) * Kn.r * dt;
   const double d1 = rdamp<FLAG>(coll);
   const double d2 = rdamp<FLAG>(2.0 / 3 * coll);
   Q[0] = rho;
@@ -342,7 +339,7 @@ __device__ __forceinline__ void relax_prim(const double (&P)[NV], double (&Q)[NV
 template <int FLAG>
 __device__ __forceinline__ double relax_cfl(const double (&P)[NV], double dt, const Recip& Kn) {
   const double nu0 = 1.0;
-  const double num = nu0 * P[0] * fsqrt1(P[3]);
+  const double num = nu0 * P[0] * fsqrt(P[3]);
   const double coll = (__builtin_expect(mk_in(num), 1) ? Kn.exact(num) : div_ieee(num, Kn.y)) * dt;
   return 0.5 * (1 - rdamp<FLAG>(2.0 / 3 * coll));
 }
@@ -422,8 +419,8 @@ __device__ __forceinline__ double hll(const double (&PL_)[NV], const double (&PR
 #pragma unroll
     for (int n = 0; n < NV; n++) { PL[n] = PL_[n]; PR[n] = PR_[n]; }
   }
-  const double cR = fsqrt1(20.0 / 3 * PR[3]);
-  const double cL = fsqrt1(20.0 / 3 * PL[3]);
+  const double cR = fsqrt(20.0 / 3 * PR[3]);
+  const double cL = fsqrt(20.0 / 3 * PL[3]);
   cons_flux_x(PL, UL, fL);
   cons_flux_x(PR, UR, fR);
   const double vR = PR[1], vL = PL[1];

@@ -85,8 +85,10 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   const bool col_out = lane >= 2 && lane <= 29 && C >= NG && C <= nxp - 1 - NG;
   const bool ylane = lane >= 2 && lane <= 29;        // owners of this strip's y faces
   const double dtdx = dt / B.dx, dtdy = dt / B.dy;
+#if !MBM_FAST_ARITH
   const Recip rdx(B.dx), rdy(B.dy);   // dx, dy in the safe range (checked at creation)
   const double hdx = 0.5 * B.dx, hdy = 0.5 * B.dy;
+#endif
   double lamx = 0.0, lamy = 0.0, prod = 0.0;
   bool nonfinite = false;
 
@@ -159,6 +161,20 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     const bool face_now = r >= rs + 3;
     if (r >= rs + 2) {
       double hi[NV], S[NV];
+#if MBM_FAST_ARITH
+      // the face states P -+ (dy/2) (L/dy) are P -+ L/2: dy cancels
+#pragma unroll
+      for (int n = 0; n < NV; n++) {
+        const double pm = win.P[sm2][n][lane], p0 = win.P[sm1][n][lane], pp = win.P[s0][n][lane];
+        S[n] = limit<LIM>(p0 - pm, pp - p0);
+      }
+#pragma unroll
+      for (int n = 0; n < NV; n++) {
+        const double p0 = win.P[sm1][n][lane];
+        hi[n] = fma(-0.5, S[n], p0);
+        G[n] = fma(0.5, S[n], p0);            // lower state of the next face, parked in G
+      }
+#else
       bool sbad = false;
 #pragma unroll
       for (int n = 0; n < NV; n++) {
@@ -180,6 +196,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         hi[n] = p0 - hdy * S[n];
         G[n] = p0 + hdy * S[n];               // lower state of the next face, parked in G
       }
+#endif
       if (face_now && ylane) {
         double lo[NV];
 #pragma unroll
@@ -200,13 +217,27 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     if (HEUN == 1) cp_async_wait_one();     // this row's Data0 has landed
     if (J >= w.J0 && J < w.J1) {
       double P0[NV], Sx[NV], lo[NV], hi[NV], F[NV];
+      // the right-hand difference of a lane is its right neighbour's left-hand one (the
+      // same subtraction of the same operands), passed down instead of recomputed
+#if MBM_FAST_ARITH
+#pragma unroll
+      for (int n = 0; n < NV; n++) {
+        P0[n] = win.P[sm2][n][lane];
+        const double d1 = P0[n] - __shfl_up_sync(0xffffffffu, P0[n], 1);
+        Sx[n] = limit<LIM>(d1, __shfl_down_sync(0xffffffffu, d1, 1));
+      }
+#pragma unroll
+      for (int n = 0; n < NV; n++) {        // P -+ L/2, as for the y faces
+        lo[n] = fma(0.5, Sx[n], P0[n]);
+        hi[n] = __shfl_down_sync(0xffffffffu, fma(-0.5, Sx[n], P0[n]), 1);
+      }
+#else
       bool xbad = false;
 #pragma unroll
       for (int n = 0; n < NV; n++) {
         P0[n] = win.P[sm2][n][lane];
-        const double pl = __shfl_up_sync(0xffffffffu, P0[n], 1);
-        const double pr = __shfl_down_sync(0xffffffffu, P0[n], 1);
-        const double L = limit<LIM>(P0[n] - pl, pr - P0[n]);
+        const double d1 = P0[n] - __shfl_up_sync(0xffffffffu, P0[n], 1);
+        const double L = limit<LIM>(d1, __shfl_down_sync(0xffffffffu, d1, 1));
         xbad |= !mk_in(L);
         Sx[n] = mk_div(L, rdx.y, rdx.r);
       }
@@ -223,6 +254,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         lo[n] = P0[n] + hdx * Sx[n];
         hi[n] = __shfl_down_sync(0xffffffffu, P0[n] - hdx * Sx[n], 1);
       }
+#endif
 #pragma unroll
       for (int n = 0; n < NV; n++) F[n] = 0.0;
       if (lane >= 1 && lane <= 29) {

@@ -140,24 +140,19 @@ def test_fast_batch_equals_fast_alone():
 
 def test_fast_reciprocal_and_root_within_one_ulp():
     """The refined reciprocal and square root of the fast kernel against the correctly
-    rounded 1/x and sqrt(x), over 2e6 values with exponents in [-300, 300]: within one
-    unit in the last place; the root without its last correction (wave speeds,
-    collision frequencies) within a relative 5e-16."""
+    rounded 1/x and sqrt(x), over 2e6 values with exponents in [-300, 300]."""
     import ctypes
     import torch
     rng = np.random.default_rng(0)
     n = 2_000_000
     x = np.ldexp(rng.uniform(1.0, 2.0, n), rng.integers(-300, 301, n))
     xd = torch.tensor(x, device="cuda")
-    out = torch.empty(3 * n, dtype=torch.float64, device="cuda")
+    out = torch.empty(2 * n, dtype=torch.float64, device="cuda")
     assert _abi.lib().mbm_fastmath_check(ctypes.c_void_p(xd.data_ptr()), n, ctypes.c_void_p(out.data_ptr())) == 0
-    o = out.cpu().numpy().reshape(n, 3)
+    o = out.cpu().numpy().reshape(n, 2)
     r, q = 1.0 / x, np.sqrt(x)
     ulp_r = np.abs(o[:, 0] - r) / np.spacing(r)
     ulp_q = np.abs(o[:, 1] - q) / np.spacing(q)
-    rel_q1 = np.abs(o[:, 2] - q) / q
-    print("fast reciprocal: max %.2f ulp, %.3f%% not correctly rounded; root: max %.2f ulp, %.3f%%; "
-          "uncorrected root: max rel %.3g" %
-          (ulp_r.max(), 100 * np.mean(ulp_r > 0), ulp_q.max(), 100 * np.mean(ulp_q > 0), rel_q1.max()))
+    print("fast reciprocal: max %.2f ulp, %.3f%% not correctly rounded; root: max %.2f ulp, %.3f%%" %
+          (ulp_r.max(), 100 * np.mean(ulp_r > 0), ulp_q.max(), 100 * np.mean(ulp_q > 0)))
     assert ulp_r.max() <= 1.0 and ulp_q.max() <= 1.0
-    assert rel_q1.max() <= 5e-16
