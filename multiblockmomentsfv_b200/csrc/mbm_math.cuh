@@ -277,7 +277,7 @@ template <int FLAG>
 __device__ __forceinline__ double rdamp(double z) {
   if (FLAG == -1 || FLAG == 0) return fdiv(1 + 0.5 * z - 0.25 * z * z, 1 + z + 0.25 * z * z);
   if (FLAG == 1) return fdiv(1 + z, 1 + z + 0.25 * z * z);
-  if (FLAG == 2) return fdiv(1 + 0.5 * z, 1 + 0.5 * z);
+  if (FLAG == 2) return MBM_FAST_ARITH ? 1.0 : fdiv(1 + 0.5 * z, 1 + 0.5 * z);   // the identity
   return fdiv(1.0, 1 + 0.5 * z);
 }
 
@@ -332,6 +332,26 @@ __device__ __forceinline__ void relax_prim(const double (&P)[NV], double (&Q)[NV
   Q[6] = d1 * (P[6] - th) + th;
   Q[7] = d2 * P[7];
   Q[8] = d2 * P[8];
+}
+#endif
+
+#if MBM_FAST_ARITH
+// relax<2>(Primitive(U)) in moment form (fast arithmetic): flag 2 leaves T and q as
+// they are (R = 1), so only the push of the velocity by g = dt F changes the moments:
+//   U1 + rho g,  E + g (U1 + rho g/2),  U4 + g (2 U1 + rho g),  U5 + g U2,
+//   U7 + g (E + U4 + g (3 U1 + rho g)/2),  U8 + g (U5 + g U2/2)   (E = U3)
+// -- no Primitive, no division
+__device__ __forceinline__ void push_moments(const double (&U)[NV], double g, double (&R)[NV]) {
+  const double rg = U[0] * g;
+  R[0] = U[0];
+  R[1] = U[1] + rg;
+  R[2] = U[2];
+  R[3] = fma(g, fma(0.5, rg, U[1]), U[3]);
+  R[4] = fma(g, fma(2.0, U[1], rg), U[4]);
+  R[5] = fma(g, U[2], U[5]);
+  R[6] = U[6];
+  R[7] = fma(g, U[3] + U[4] + 0.5 * g * fma(3.0, U[1], rg), U[7]);
+  R[8] = fma(g, fma(0.5 * g, U[2], U[5]), U[8]);
 }
 #endif
 
@@ -404,14 +424,17 @@ __device__ __forceinline__ void cons_flux_x(const double (&P)[NV], double (&U)[N
 // FnumHLLE (src/Flux.c:308-379) in primitive form (fast arithmetic): the Grad-13
 // flux straight from the face states -- no Conservative -> Primitive round trip and
 // no rotations (a y face swaps the x and y components, which is what the rotation
-// to the normal (0,1) amounts to); c = 2 sqrt(5/3 theta) as sqrt(20/3 theta); the
-// combination (lamR fL - lamL fR + lamL lamR (UR - UL)) / alpha with its three
-// coefficients formed once.  Mathematically the bitwise version below; the rounding
-// differs.
+// to the normal (0,1) amounts to); c = 2 sqrt(5/3 theta) as sqrt(20/3 theta).  The
+// wave speeds and the coefficients of
+//   (lamR fL - lamL fR + lamL lamR (UR - UL)) / alpha
+// come first, then each side's moments and flux are formed and added in turn, so one
+// side's vectors are live at a time (alpha = 0, both speeds 0: the mean of the two
+// fluxes, coefficients 1/2, -1/2, 0).  Mathematically the bitwise version below; the
+// rounding differs.
 template <int DIR>
 __device__ __forceinline__ double hll(const double (&PL_)[NV], const double (&PR_)[NV],
                                       double (&flx)[NV]) {
-  double PL[NV], PR[NV], UL[NV], UR[NV], fL[NV], fR[NV];
+  double PL[NV], PR[NV];
   if (DIR == 2) {
     mbm_adj::swap_xy(PL_, PL);
     mbm_adj::swap_xy(PR_, PR);
@@ -421,23 +444,22 @@ __device__ __forceinline__ double hll(const double (&PL_)[NV], const double (&PR
   }
   const double cR = fsqrt(20.0 / 3 * PR[3]);
   const double cL = fsqrt(20.0 / 3 * PL[3]);
-  cons_flux_x(PL, UL, fL);
-  cons_flux_x(PR, UR, fR);
   const double vR = PR[1], vL = PL[1];
   const double cMax = fabs(0.5 * (vL + vR)) + rmax(cR, cL);
   const double lamL = rmin(vL - cL, 0.0);
   const double lamR = rmax(vR + cR, 0.0);
   const double alph = lamR - lamL;
-  double f[NV];
-  if (alph > 0.0) {
-    const double ra = frcp(alph);
-    const double ca = lamR * ra, cb = lamL * ra, cc = lamL * ca;
+  const double ra = frcp(alph);
+  const bool pos = alph > 0.0;
+  const double a = lamR * ra, b = lamL * ra;
+  const double ca = pos ? a : 0.5, cb = pos ? b : -0.5, cc = pos ? lamL * a : 0.0;
+  double U[NV], F[NV], f[NV];
+  cons_flux_x(PL, U, F);
 #pragma unroll
-    for (int n = 0; n < NV; n++) f[n] = fma(cc, UR[n] - UL[n], fma(-cb, fR[n], ca * fL[n]));
-  } else {
+  for (int n = 0; n < NV; n++) f[n] = fma(-cc, U[n], ca * F[n]);
+  cons_flux_x(PR, U, F);
 #pragma unroll
-    for (int n = 0; n < NV; n++) f[n] = 0.5 * (fL[n] + fR[n]);
-  }
+  for (int n = 0; n < NV; n++) f[n] = fma(cc, U[n], fma(-cb, F[n], f[n]));
   if (DIR == 2) {
     mbm_adj::swap_xy(f, flx);
   } else {

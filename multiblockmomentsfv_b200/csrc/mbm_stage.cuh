@@ -269,8 +269,17 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         const long long idx = (long long)J * pitch + C + 1;
         double U[NV], Q[NV], R[NV];
         load_cell(in, plane, idx, U);
+#if MBM_FAST_ARITH
+        if (HEUN == 1) {
+          push_moments(U, dt * Fx, R);        // relax<2>: the force push alone
+        } else {
+          primitive(U, Q);
+          relax<0>(Q, R, dt, Kn, Fx);
+        }
+#else
         primitive(U, Q);
         relax<2 * HEUN>(Q, R, dt, Kn, Fx);
+#endif
         if (HEUN == 1) {
           double R0[NV];
 #pragma unroll
