@@ -8,10 +8,6 @@
 // the bitwise kernel's unfused arithmetic needs more registers than the fast one: two
 // CTAs per SM (255 registers, no spills) run it 2 % faster than three (168, spilling)
 #define STAGE_MIN_CTAS 2
-// and one work item per one-warp CTA runs it 2.6 % faster than the persistent grid
-// (1.15e9 against 1.12e9 cell-updates/s at 4 x 1024^2); the fast kernel is 1 % faster
-// with the persistent grid
-#define STAGE_PER_ITEM 1
 #include "mbm_stage.cuh"   // the stage kernel in namespace mbm::bitwise
 
 namespace mbm {

@@ -329,28 +329,11 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   }
 }
 
-#ifndef STAGE_PER_ITEM
-#define STAGE_PER_ITEM 0
-#endif
-#if STAGE_PER_ITEM
-// One work item per one-warp CTA (item = blockIdx.x, the same in every lane, so that
-// everything derived from the item can live in uniform registers); the hardware's
-// block scheduler hands out the items as CTAs finish.
-constexpr int STAGE_THREADS = 32;
-constexpr int STAGE_SMEM = (int)sizeof(WarpWindow);
-
-template <int HEUN, int LIM>
-__global__ void __launch_bounds__(32, STAGE_MIN_CTAS * STAGE_WARPS) stage_kernel(const StageArgs a) {
-  extern __shared__ __align__(16) unsigned char stage_smem[];
-  stage_item<HEUN, LIM>(a, a.work[blockIdx.x], threadIdx.x, *reinterpret_cast<WarpWindow*>(stage_smem));
-}
-#else
 // Persistent grid (as many CTAs as fit on the SMs); every warp takes the next work
 // item from a counter until the table is exhausted, so uneven blocks and the last
 // wave balance themselves.
 // the windows live in dynamic shared memory (STAGE_SMEM bytes, above the 48 KB a static
 // allocation may take)
-constexpr int STAGE_THREADS = 32 * STAGE_WARPS;
 constexpr int STAGE_SMEM = (int)sizeof(WarpWindow) * STAGE_WARPS;
 
 template <int HEUN, int LIM>
@@ -366,7 +349,6 @@ __global__ void __launch_bounds__(32 * STAGE_WARPS, STAGE_MIN_CTAS) stage_kernel
     stage_item<HEUN, LIM>(a, a.work[w], lane, win[warp]);
   }
 }
-#endif
 
 template <int HEUN, int LIM>
 static void smem_attr() {
@@ -391,20 +373,18 @@ int stage_ctas_per_sm() {
     }
   }
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<1, 4>, STAGE_THREADS, STAGE_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<1, 4>, 32 * STAGE_WARPS, STAGE_SMEM);
   return n > 0 ? n : 1;
 }
 
 template <int HEUN>
 static cudaError_t launch_stage_lim(int lim, const StageArgs& a, int grid, cudaStream_t s) {
-  if (STAGE_PER_ITEM) grid = a.nwork;     // one CTA per work item
-  if (grid <= 0) return cudaSuccess;
   switch (lim) {
-    case 0: stage_kernel<HEUN, 0><<<grid, STAGE_THREADS, STAGE_SMEM, s>>>(a); break;
-    case 1: stage_kernel<HEUN, 1><<<grid, STAGE_THREADS, STAGE_SMEM, s>>>(a); break;
-    case 2: stage_kernel<HEUN, 2><<<grid, STAGE_THREADS, STAGE_SMEM, s>>>(a); break;
-    case 3: stage_kernel<HEUN, 3><<<grid, STAGE_THREADS, STAGE_SMEM, s>>>(a); break;
-    default: stage_kernel<HEUN, 4><<<grid, STAGE_THREADS, STAGE_SMEM, s>>>(a); break;
+    case 0: stage_kernel<HEUN, 0><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
+    case 1: stage_kernel<HEUN, 1><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
+    case 2: stage_kernel<HEUN, 2><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
+    case 3: stage_kernel<HEUN, 3><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
+    default: stage_kernel<HEUN, 4><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
   }
   return cudaGetLastError();
 }
