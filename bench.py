@@ -507,7 +507,7 @@ def main():
             "config": {"workload": f"scaled square4: 4 blocks x {a.n}^2 cells ({cells} cells), open outer "
                                    "edges, Kn=0.01, R13=1, harmonic, CFL 0.95, FP64, "
                                    + ("fast mode (within 1e-10 of the reference after one step, 1e-8 at t_end; "
-                                      "measured 5e-13 at t=0.3)" if a.mode == "fast" else "bitwise mode"),
+                                      "measured 4e-13 at t=0.3)" if a.mode == "fast" else "bitwise mode"),
                        "mode": a.mode, "cells": cells, "rejected_attempts": nrej,
                        "l2": "working set 3 layers x 4 blocks x 9 planes = "
                              f"{3 * 9 * 8 * sum(b.cells for b in d.blocks) / 1e6:.0f} MB > 126 MB L2, no flush",
