@@ -93,8 +93,12 @@ struct Recip {        // 1/y for a denominator shared by several quotients
 #else
     r = __drcp_rn(y_);
 #endif
+#if MBM_FAST_ARITH
+    bad = false;      // no range check: quotients are x * r, no IEEE fallback
+#else
     const unsigned e = (unsigned)(__double_as_longlong(y_) >> 52) & 0x7ffu;
     bad = e - 543u > 960u;
+#endif
   }
   __device__ __forceinline__ Recip(double y_, double r_) {   // r_ = RN(1/y_), y_ in range
     y = y_;

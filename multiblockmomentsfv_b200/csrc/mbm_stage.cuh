@@ -90,7 +90,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   const double hdx = 0.5 * B.dx, hdy = 0.5 * B.dy;
 #endif
   double lamx = 0.0, lamy = 0.0, prod = 0.0;
-  bool nonfinite = false;
+  int expmax = 0;     // largest exponent field (high word & 0x7ff00000) written: all ones = NaN or inf
 
   // The march: iteration r forms the primitives of row r, the y slope of row r-1
   // and the y face (r-2 | r-1), then finishes row J = r-2 (x face, update).
@@ -223,7 +223,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
 #pragma unroll
       for (int n = 0; n < NV; n++) {
         P0[n] = win.P[sm2][n][lane];
-        const double d1 = P0[n] - __shfl_up_sync(0xffffffffu, P0[n], 1);
+        const double d1 = P0[n] - win.P[sm2][n][(lane + 31) & 31];   // left neighbour (lane 0: unused)
         Sx[n] = limit<LIM>(d1, __shfl_down_sync(0xffffffffu, d1, 1));
       }
 #pragma unroll
@@ -236,7 +236,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
 #pragma unroll
       for (int n = 0; n < NV; n++) {
         P0[n] = win.P[sm2][n][lane];
-        const double d1 = P0[n] - __shfl_up_sync(0xffffffffu, P0[n], 1);
+        const double d1 = P0[n] - win.P[sm2][n][(lane + 31) & 31];   // left neighbour (lane 0: unused)
         const double L = limit<LIM>(d1, __shfl_down_sync(0xffffffffu, d1, 1));
         xbad |= !mk_in(L);
         Sx[n] = mk_div(L, rdx.y, rdx.r);
@@ -298,7 +298,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
           v -= dtdx * F[n];
           if (HEUN == 1) v = 0.5 * v;
           out[n * plane + idx] = v;
-          nonfinite |= (__double2hiint(v) & 0x7ff00000) == 0x7ff00000;
+          expmax = max(expmax, __double2hiint(v) & 0x7ff00000);
         }
       }
     }
@@ -320,7 +320,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     prod = fmax(prod, __shfl_xor_sync(0xffffffffu, prod, o));
   }
   // failure detection: a NaN or infinity in a written cell marks the case
-  if (__any_sync(0xffffffffu, nonfinite) && lane == 0) atomicOr(&a.cases[B.case_id].nonfinite, 1);
+  if (__any_sync(0xffffffffu, expmax == 0x7ff00000) && lane == 0) atomicOr(&a.cases[B.case_id].nonfinite, 1);
   if (lane == 0) {
     unsigned long long* slot = a.lam + ((size_t)w.blk * 2 + HEUN) * 3;
     if (lamx > 0.0) atomicMax(slot + 0, (unsigned long long)__double_as_longlong(lamx));
