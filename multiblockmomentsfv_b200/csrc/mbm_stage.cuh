@@ -217,6 +217,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     if (HEUN == 1) cp_async_wait_one();     // this row's Data0 has landed
     if (J >= w.J0 && J < w.J1) {
       double P0[NV], Sx[NV], lo[NV], hi[NV], F[NV];
+      __syncwarp();   // the window row is read across lanes below (other lanes wrote it)
       // the right-hand difference of a lane is its right neighbour's left-hand one (the
       // same subtraction of the same operands), passed down instead of recomputed
 #if MBM_FAST_ARITH
