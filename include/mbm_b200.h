@@ -252,8 +252,8 @@ int mbm_ghost_map(const mbm_block_desc *blocks, int nblocks, int *entries, int c
  * the caller owns, allocating no device memory: no cudaMalloc, cudaFree or
  * allocating library routine is called.  No counterpart in the reference (its
  * Update allocates nothing on a GPU because it has none); it exists for callers
- * that cannot allocate: a framework whose memory pool owns the GPU, code running
- * inside CUDA-graph capture, loops that fix every allocation at start-up.
+ * that cannot allocate: a framework whose memory pool owns the GPU, real-time
+ * loops that fix every allocation at start-up.
  *
  * in, data0 and out are device arrays in this library's plane layout: blocks one
  * after another; block b has 9 planes (one per moment) of (ny+6) rows x pitch

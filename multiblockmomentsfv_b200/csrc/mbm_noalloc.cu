@@ -4,9 +4,8 @@
 //
 // Some callers cannot allocate device memory at all: a host framework whose
 // memory pool owns the whole GPU (any cudaMalloc outside the pool breaks its
-// accounting or fails), code that runs between the capture calls of a CUDA graph,
-// where cudaMalloc is not allowed, and real-time or certified loops that fix
-// every allocation at start-up.  They hold their own moment buffers and only need
+// accounting or fails), and real-time or certified loops that fix every
+// allocation at start-up.  They hold their own moment buffers and only need
 // the computation.  The context API (mbm_create) allocates; this entry point does
 // not.
 //

@@ -1,8 +1,8 @@
 """mbm_stage_noalloc -- one Heun stage on device buffers the caller owns, with the
 kernel's scratch in a fixed device array -- against the allocating context path
 (mbm_update), through the C ABI.  Callers of it cannot allocate device memory (a
-memory pool owns the GPU, or the call runs inside CUDA-graph capture); here the
-test plays that caller and owns the buffers (torch tensors).
+memory pool owns the GPU, or every allocation is fixed at start-up); here the test
+plays that caller and owns the buffers (torch tensors).
 
 Two different stage calls in a row, then the first again: the shared scratch
 keeps the previous call's contents, so a call that failed to clear it would show.
