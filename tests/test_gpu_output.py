@@ -42,12 +42,16 @@ def test_writer_from_device_writes_identical_files(tmp_path):
     assert ok and mx == 0.0, msg
 
 
-def test_nan_in_state_is_reported():
+@pytest.mark.parametrize("mode,bad,comp", [("exact", np.nan, 3), ("fast", np.nan, 3), ("fast", -np.inf, 7),
+                                           ("exact", -np.nan, 0)])
+def test_nan_in_state_is_reported(mode, bad, comp):
+    """A NaN or infinity (either sign) in one moment of one cell ends the step loop
+    with MBM_ENONFINITE in both arithmetic modes."""
     d = H.quadrant_deck(32, Kn=0.01)
-    with solver.Solver(d, sc.Scenario.seeded_quadrant(2)) as s:
+    with solver.Solver(d, sc.Scenario.seeded_quadrant(2), mode=mode) as s:
         s.initialise()
         U = s.download(solver.L_DATA, 1)
-        U[10, 12, 3] = np.nan
+        U[10, 12, comp] = bad
         s.upload(solver.L_DATA, 1, U)
         with pytest.raises(_abi.MBMError) as e:
             s.steps(0.0, 0.05)
@@ -58,11 +62,12 @@ def test_nan_in_state_is_reported():
         assert n > 0 and abs(t - 0.01) < 1e-15
 
 
-def test_batch_nonfinite_case_stops_alone():
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_batch_nonfinite_case_stops_alone(mode):
     """In a batch, a case that goes non-finite stops with MBM_ENONFINITE while the
     others run to the end with the results they have alone."""
     cases = [(H.quadrant_deck(24, Kn=0.01), sc.Scenario.seeded_quadrant(k)) for k in range(3)]
-    with solver.BatchSolver(cases) as bs:
+    with solver.BatchSolver(cases, mode=mode) as bs:
         bs.initialise()
         U = bs.download(solver.L_DATA, 1, 2)
         U[8, 9, 0] = np.inf
@@ -78,7 +83,7 @@ def test_batch_nonfinite_case_stops_alone():
         assert ns[1] == 0 and abs(t[0] - 0.02) < 1e-15 and abs(t[2] - 0.02) < 1e-15
         ref = [bs.download(solver.L_DATA, k, b) for k in (0, 2) for b in range(4)]
     for i, k in enumerate((0, 2)):
-        with solver.Solver(cases[k][0], cases[k][1]) as s:
+        with solver.Solver(cases[k][0], cases[k][1], mode=mode) as s:
             s.initialise()
             s.steps(0.0, 0.02)
             for b in range(4):
