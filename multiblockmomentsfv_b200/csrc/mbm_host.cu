@@ -128,8 +128,10 @@ struct mbm_ctx {
   // adjoint work space (allocated on first use)
   double* adj_buf[8] = {nullptr};   // two adjoint layers, primitives, 4 face-adjoint layers, spare
   double* adj_ckpt = nullptr;
-  double* adj_seg = nullptr;         // DATA states of one checkpoint segment
-  double* adj_segT = nullptr;        // their stage-1 (TMP) states
+  double* adj_seg[2] = {nullptr};    // DATA states of a checkpoint segment (two: recomputation of
+  double* adj_segT[2] = {nullptr};   //   the next one beside the reversal of this one); stage-1 states
+  cudaStream_t adj_rstream = nullptr;   // the recomputation stream (low priority)
+  cudaEvent_t adj_ready[2] = {nullptr}, adj_free[2] = {nullptr}, adj_start = nullptr;
   double* adj_dtlog = nullptr;
   double* adj_scal = nullptr;       // [0] dJ/dKn, [1] J
   double* adj_dtrep = nullptr;      // dt values of mbm_replay
@@ -764,8 +766,14 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   cudaFree(c->dqueue);
   for (int k = 0; k < 8; k++) cudaFree(c->adj_buf[k]);
   cudaFree(c->adj_ckpt);
-  cudaFree(c->adj_seg);
-  cudaFree(c->adj_segT);
+  for (int k = 0; k < 2; k++) {
+    cudaFree(c->adj_seg[k]);
+    cudaFree(c->adj_segT[k]);
+    if (c->adj_ready[k]) cudaEventDestroy(c->adj_ready[k]);
+    if (c->adj_free[k]) cudaEventDestroy(c->adj_free[k]);
+  }
+  if (c->adj_start) cudaEventDestroy(c->adj_start);
+  if (c->adj_rstream) cudaStreamDestroy(c->adj_rstream);
   cudaFree(c->adj_dtlog);
   cudaFree(c->adj_dtrep);
   cudaFree(c->adj_part);
@@ -1154,16 +1162,31 @@ static int adj_alloc(mbm_ctx* c, int nsteps, int every) {
     int st = wait_stream(c);
     if (st) return st;
   }
+  if (!c->adj_rstream) {
+    int lo = 0, hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));    // lo: the least urgent
+    CK(cudaStreamCreateWithPriority(&c->adj_rstream, cudaStreamNonBlocking, lo));
+    for (int k = 0; k < 2; k++) {
+      CK(cudaEventCreateWithFlags(&c->adj_ready[k], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->adj_free[k], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&c->adj_start, cudaEventDisableTiming));
+  }
   if (nsteps > c->adj_nsteps || every != c->adj_every) {
     cudaFree(c->adj_ckpt);
-    cudaFree(c->adj_seg);
-  cudaFree(c->adj_segT);
     cudaFree(c->adj_dtlog);
-    c->adj_ckpt = c->adj_seg = c->adj_segT = c->adj_dtlog = nullptr;
+    c->adj_ckpt = c->adj_dtlog = nullptr;
+    for (int k = 0; k < 2; k++) {
+      cudaFree(c->adj_seg[k]);
+      cudaFree(c->adj_segT[k]);
+      c->adj_seg[k] = c->adj_segT[k] = nullptr;
+    }
     const int nck = nsteps / every + 1;
     CK(cudaMalloc(&c->adj_ckpt, sizeof(double) * c->layer_elems * nck));
-    CK(cudaMalloc(&c->adj_seg, sizeof(double) * c->layer_elems * (every + 1)));
-    CK(cudaMalloc(&c->adj_segT, sizeof(double) * c->layer_elems * every));
+    for (int k = 0; k < 2; k++) {
+      CK(cudaMalloc(&c->adj_seg[k], sizeof(double) * c->layer_elems * (every + 1)));
+      CK(cudaMalloc(&c->adj_segT[k], sizeof(double) * c->layer_elems * every));
+    }
     CK(cudaMalloc(&c->adj_dtlog, sizeof(double) * nsteps));
     c->adj_nsteps = nsteps;
     c->adj_every = every;
@@ -1293,25 +1316,51 @@ extern "C" int mbm_adjoint_run(mbm_ctx* c, double* t, int nsteps, int every, dou
   CK(cudaMemsetAsync(c->adj_scal, 0, sizeof(double) * 2, c->stream));
   CK(cudaMemsetAsync(lam, 0, bytes, c->stream));
   CK(adjoint_functional(c->dblk, c->nblk, c->buf[h.cur], lam, adj_threads(c), c->adj_part, c->adj_scal + 1, c->stream));
-  // reverse sweep over segments [s*every, min((s+1)*every, n))
+  // reverse sweep over segments [s*every, min((s+1)*every, n)).  The recomputation of
+  // segment s-1 from its checkpoint (frozen-dt forward steps, on the low-priority
+  // recomputation stream, into the other of the two segment buffers) runs beside the
+  // reversal of segment s on the context stream: the forward kernels are FP64-bound,
+  // the adjoint passes wait on their neighbour loads, so the two share the SMs.  The
+  // recomputation touches the case record, the work counters and the CFL maxima, the
+  // reversal only the adjoint buffers.  Events order buffer reuse: recomputing into a
+  // buffer waits until the reversal that read it is done (adj_free), reversing a
+  // segment waits for its recomputation (adj_ready).
   const int cur0 = h.cur;
   if ((st = frozen_begin(c))) return st;
-  for (int s = (n - 1) / every; s >= 0; s--) {
-    const int a = s * every, b = std::min(n, a + every);
-    CK(cudaMemcpyAsync(c->adj_seg, c->adj_ckpt + (size_t)s * c->layer_elems, bytes, cudaMemcpyDeviceToDevice,
-                       c->stream));
-    // recompute the segment's states and stage-1 states (the last step's stage 1 only)
-    for (int k = a; k < b; k++)
-      if ((st = frozen_step(c, c->adj_seg + (size_t)(k - a) * c->layer_elems,
-                            k < b - 1 ? c->adj_seg + (size_t)(k - a + 1) * c->layer_elems : nullptr,
-                            c->adj_dtlog + k, c->adj_segT + (size_t)(k - a) * c->layer_elems)))
-        return st;
+  CK(cudaEventRecord(c->adj_start, c->stream));
+  CK(cudaStreamWaitEvent(c->adj_rstream, c->adj_start, 0));
+  bool used[2] = {false, false};
+  auto recompute = [&](int sg) -> int {
+    const int a = sg * every, b = std::min(n, a + every), k2 = sg & 1;
+    std::swap(c->stream, c->adj_rstream);      // frozen_step issues on c->stream
+    int rc = MBM_OK;
+    if (used[k2] && cudaStreamWaitEvent(c->stream, c->adj_free[k2], 0) != cudaSuccess) rc = MBM_ECUDA;
+    if (!rc && cudaMemcpyAsync(c->adj_seg[k2], c->adj_ckpt + (size_t)sg * c->layer_elems, bytes,
+                               cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+      rc = MBM_ECUDA;
+    // the segment's states and stage-1 states (the last step's stage 1 only)
+    for (int k = a; !rc && k < b; k++)
+      rc = frozen_step(c, c->adj_seg[k2] + (size_t)(k - a) * c->layer_elems,
+                       k < b - 1 ? c->adj_seg[k2] + (size_t)(k - a + 1) * c->layer_elems : nullptr,
+                       c->adj_dtlog + k, c->adj_segT[k2] + (size_t)(k - a) * c->layer_elems);
+    if (!rc && cudaEventRecord(c->adj_ready[k2], c->stream) != cudaSuccess) rc = MBM_ECUDA;
+    std::swap(c->stream, c->adj_rstream);
+    used[k2] = true;
+    return rc;
+  };
+  const int nseg = (n - 1) / every + 1;
+  if ((st = recompute(nseg - 1))) return fail(c, st, "mbm_adjoint_run: recomputation failed");
+  for (int sg = nseg - 1; sg >= 0; sg--) {
+    const int a = sg * every, b = std::min(n, a + every), k2 = sg & 1;
+    if (sg > 0 && (st = recompute(sg - 1))) return fail(c, st, "mbm_adjoint_run: recomputation failed");
+    CK(cudaStreamWaitEvent(c->stream, c->adj_ready[k2], 0));
     for (int k = b - 1; k >= a; k--) {
-      if ((st = adj_step(c, c->adj_seg + (size_t)(k - a) * c->layer_elems,
-                         c->adj_segT + (size_t)(k - a) * c->layer_elems, dts[k], lam, lam2)))
+      if ((st = adj_step(c, c->adj_seg[k2] + (size_t)(k - a) * c->layer_elems,
+                         c->adj_segT[k2] + (size_t)(k - a) * c->layer_elems, dts[k], lam, lam2)))
         return st;
       std::swap(lam, lam2);
     }
+    CK(cudaEventRecord(c->adj_free[k2], c->stream));
   }
   h.cur = cur0;
   h.done = 1;
