@@ -126,7 +126,7 @@ struct mbm_ctx {
   double* shard_cfl = nullptr;
   std::vector<int> shard_dir_off, shard_nt;   // Dirichlet rows of every block's edges (whole table)
   // adjoint work space (allocated on first use)
-  double* adj_buf[8] = {nullptr};   // two adjoint layers, primitives, 4 face-adjoint layers, spare
+  double* adj_buf[8] = {nullptr};   // two adjoint layers, stage-1 adjoint, primitives, 4 face-adjoint layers
   double* adj_ckpt = nullptr;
   double* adj_seg[2] = {nullptr};    // DATA states of a checkpoint segment (two: recomputation of
   double* adj_segT[2] = {nullptr};   //   the next one beside the reversal of this one); stage-1 states
@@ -1138,8 +1138,8 @@ static long long adj_threads(mbm_ctx* c) {
 }
 
 static int adj_alloc(mbm_ctx* c, int nsteps, int every) {
-  if (!c->adj_buf[0])
-    for (int k = 0; k < 8; k++) CK(cudaMalloc(&c->adj_buf[k], sizeof(double) * c->layer_elems));
+  for (int k = 0; k < 8; k++)      // each one missing (mbm_replay may have made the first)
+    if (!c->adj_buf[k]) CK(cudaMalloc(&c->adj_buf[k], sizeof(double) * c->layer_elems));
   if (!c->adj_scal) CK(cudaMalloc(&c->adj_scal, sizeof(double) * 2));
   if (!c->adj_part) CK(cudaMalloc(&c->adj_part, sizeof(double) * ((adj_threads(c) + 127) / 128)));
   if (!c->adj_work) {   // row-marching work: strips of ASTRIP columns x 32-row segments of the non-ring cells
