@@ -139,6 +139,7 @@ struct mbm_ctx {
   // the row-marching adjoint pass (MBM_ADJ_MARCH=1; the three-pass one is the default)
   bool adj_march = false;
   Work* adj_work = nullptr;
+  bool adj_work_ready = false;
   int adj_nwork = 0, adj_grid = 0;
   int* adj_queue = nullptr;
   int adj_nsteps = 0, adj_every = 0, adj_nrep = 0;
@@ -846,15 +847,18 @@ extern "C" int mbm_output_fields_async(mbm_ctx* c, int block, int single, void* 
   if (!c || !host || block < 0 || block >= c->nblk) return fail(c, MBM_EINVAL, "mbm_output_fields_async: bad argument");
   CK(cudaSetDevice(c->device));
   if (!c->out_stage) {   // one payload area per block, an own stream for the copies
+    std::vector<size_t> offs;
     size_t off = 0;
     for (auto& d : c->hblk) {
-      c->out_off.push_back(off);
+      offs.push_back(off);
       off += ((size_t)(d.nxp - 4) * (d.nyp - 4) * 10 * sizeof(double) + 255) & ~(size_t)255;
     }
     CK(cudaMalloc(&c->out_stage, off));
-    CK(cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&c->out_ev, cudaEventDisableTiming));
+    c->out_off = offs;
   }
+  // each resource on its own, so that a call after a failed one completes the set
+  if (!c->out_stream) CK(cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking));
+  if (!c->out_ev) CK(cudaEventCreateWithFlags(&c->out_ev, cudaEventDisableTiming));
   const BlockDev& d = c->hblk[block];
   const size_t bytes = (size_t)(d.nxp - 4) * (d.nyp - 4) * 10 * (single ? sizeof(float) : sizeof(double));
   char* dst = (char*)c->out_stage + c->out_off[block];
@@ -1142,7 +1146,7 @@ static int adj_alloc(mbm_ctx* c, int nsteps, int every) {
     if (!c->adj_buf[k]) CK(cudaMalloc(&c->adj_buf[k], sizeof(double) * c->layer_elems));
   if (!c->adj_scal) CK(cudaMalloc(&c->adj_scal, sizeof(double) * 2));
   if (!c->adj_part) CK(cudaMalloc(&c->adj_part, sizeof(double) * ((adj_threads(c) + 127) / 128)));
-  if (!c->adj_work) {   // row-marching work: strips of ASTRIP columns x 32-row segments of the non-ring cells
+  if (!c->adj_work_ready) {   // row-marching work: strips of ASTRIP columns x 32-row segments of the non-ring cells
     const char* env = getenv("MBM_ADJ_MARCH");
     c->adj_march = env && atoi(env) == 1;
     std::vector<Work> wl;
@@ -1154,24 +1158,25 @@ static int adj_alloc(mbm_ctx* c, int nsteps, int every) {
         for (int I0 = 1; I0 <= d.nxp - 2; I0 += ASTRIP) wl.push_back(Work{b, I0, J0, J1});
       }
     }
-    c->adj_nwork = (int)wl.size();
-    CK(cudaMalloc(&c->adj_work, sizeof(Work) * std::max<size_t>(1, wl.size())));
+    if (!c->adj_work) CK(cudaMalloc(&c->adj_work, sizeof(Work) * std::max<size_t>(1, wl.size())));
     CK(cudaMemcpyAsync(c->adj_work, wl.data(), sizeof(Work) * wl.size(), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMalloc(&c->adj_queue, sizeof(int)));
-    c->adj_grid = std::max(1, std::min((c->adj_nwork + 3) / 4, c->nsm * adjoint_march_ctas()));
-    int st = wait_stream(c);
+    const int st = wait_stream(c);
     if (st) return st;
+    c->adj_work_ready = true;     // the table is complete on the device
+    c->adj_nwork = (int)wl.size();
+    c->adj_grid = std::max(1, std::min((c->adj_nwork + 3) / 4, c->nsm * adjoint_march_ctas()));
   }
+  if (!c->adj_queue) CK(cudaMalloc(&c->adj_queue, sizeof(int)));
   if (!c->adj_rstream) {
     int lo = 0, hi = 0;
     CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));    // lo: the least urgent
     CK(cudaStreamCreateWithPriority(&c->adj_rstream, cudaStreamNonBlocking, lo));
-    for (int k = 0; k < 2; k++) {
-      CK(cudaEventCreateWithFlags(&c->adj_ready[k], cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&c->adj_free[k], cudaEventDisableTiming));
-    }
-    CK(cudaEventCreateWithFlags(&c->adj_start, cudaEventDisableTiming));
   }
+  for (int k = 0; k < 2; k++) {      // each one missing
+    if (!c->adj_ready[k]) CK(cudaEventCreateWithFlags(&c->adj_ready[k], cudaEventDisableTiming));
+    if (!c->adj_free[k]) CK(cudaEventCreateWithFlags(&c->adj_free[k], cudaEventDisableTiming));
+  }
+  if (!c->adj_start) CK(cudaEventCreateWithFlags(&c->adj_start, cudaEventDisableTiming));
   if (nsteps > c->adj_nsteps || every != c->adj_every) {
     cudaFree(c->adj_ckpt);
     cudaFree(c->adj_dtlog);
