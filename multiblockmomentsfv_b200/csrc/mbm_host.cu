@@ -147,6 +147,15 @@ struct mbm_ctx {
 };
 
 // ------------------------------------------------------------------ helpers --
+// timing events of one call, destroyed on every return path
+struct LocalEvents {
+  cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+  ~LocalEvents() {
+    for (cudaEvent_t x : e)
+      if (x) cudaEventDestroy(x);
+  }
+};
+
 static int fail(mbm_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
   else g_create_error = msg;
@@ -462,21 +471,19 @@ static int autotune(mbm_ctx* c) {
   }
   int st = push_cases(c);
   if (st) return st;
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
+  LocalEvents ev;
+  CK(cudaEventCreate(&ev.e[0]));
+  CK(cudaEventCreate(&ev.e[1]));
   int best = 32;
   float best_ms = 1e30f;
   // short segments buy parallelism on small grids, long ones save warm-up rows
   for (int seg : {8, 12, 16, 24, 32, 48, 64}) {
     st = set_segments(c, seg);
     float ms = 0.f;
-    if (!st) st = time_both_stages(c, e0, e1, &ms);
-    if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
+    if (!st) st = time_both_stages(c, ev.e[0], ev.e[1], &ms);
+    if (st) return st;
     if (ms < best_ms) { best_ms = ms; best = seg; }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   for (int l = 0; l < 3; l++) CK(cudaMemsetAsync(c->buf[l], 0, sizeof(double) * c->layer_elems, c->stream));
   CK(cudaMemsetAsync(c->dlam, 0, sizeof(unsigned long long) * 6 * c->nblk, c->stream));
   for (int k = 0; k < c->ncase; k++) c->hcase[k].done = 1;
@@ -1092,7 +1099,9 @@ extern "C" int mbm_time_stage(mbm_ctx* c, int heun, double dt, int reps, double*
   int st = push_cases(c);
   if (st) return st;
   const int si = heun ? SEL_TMP : SEL_CUR, so = heun ? SEL_OTHER : SEL_TMP;
-  cudaEvent_t e0, e1;
+  LocalEvents ev;
+  cudaEvent_t& e0 = ev.e[0];
+  cudaEvent_t& e1 = ev.e[1];
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
@@ -1108,8 +1117,6 @@ extern "C" int mbm_time_stage(mbm_ctx* c, int heun, double dt, int reps, double*
   st = wait_stream(c);
   float el = 0.f;
   if (!st) CK(cudaEventElapsedTime(&el, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   if (st) return st;
   *ms = el / reps;
   return MBM_OK;
@@ -1289,7 +1296,10 @@ extern "C" int mbm_adjoint_run(mbm_ctx* c, double* t, int nsteps, int every, dou
   int st = adj_alloc(c, nsteps, every);
   if (st) return st;
   const size_t bytes = sizeof(double) * c->layer_elems;
-  cudaEvent_t e0, e1, e2;
+  LocalEvents ev;
+  cudaEvent_t& e0 = ev.e[0];
+  cudaEvent_t& e1 = ev.e[1];
+  cudaEvent_t& e2 = ev.e[2];
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   CK(cudaEventCreate(&e2));
@@ -1379,9 +1389,6 @@ extern "C" int mbm_adjoint_run(mbm_ctx* c, double* t, int nsteps, int every, dou
   float f_ms = 0.f, a_ms = 0.f;
   CK(cudaEventElapsedTime(&f_ms, e0, e1));
   CK(cudaEventElapsedTime(&a_ms, e1, e2));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaEventDestroy(e2);
   if (J) *J = sc[1];
   if (grad_Kn) *grad_Kn = sc[0];
   if (ms) { ms[0] = f_ms; ms[1] = a_ms; }
