@@ -289,7 +289,10 @@ int mbm_stage_noalloc(const mbm_block_desc *blocks, int nblocks, const double *i
  * (ghost cells zero), *grad_Kn = dJ/dKn, dts[nsteps] (may be NULL) the frozen dt
  * sequence, ms[0..1] (may be NULL) the forward and the adjoint device times.  *t
  * advances to the forward run's end.  Needs a single-case context created with
- * mbm_params.adjoint = 1. */
+ * mbm_params.adjoint = 1.  Device memory it holds after the first call: 8 layers
+ * of work space, nsteps/every + 1 checkpoints and two segments of 2*every + 1 layers
+ * (the next segment is recomputed beside the reversal of the current one), i.e.
+ * about (nsteps/every + 4*every + 11) layers of the context's size. */
 int mbm_adjoint_run(mbm_ctx *ctx, double *t, int nsteps, int every, double CFLreg, double *J,
                     double *grad, double *grad_Kn, double *dts, double *ms);
 
