@@ -47,7 +47,8 @@ struct WarpWindow {
   double P[3][NV][32];
   double lo[NV][32];
   double G[NV][32];
-  double D0[2][NV][32];   // stage 2: Data0 of the next two update rows (asynchronous copies)
+  double Ua[NV][32];      // stage 2: the moments of the next row (asynchronous copies)
+  double D0a[NV][32];     // stage 2: Data0 of the next update row (asynchronous copies)
 };
 
 // per-thread asynchronous 8-byte copy global -> shared (cp.async), and its groups
@@ -99,20 +100,32 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   // Stage 1 loads the moments of row r+1 while it works on row r (nine registers,
   // which stage 2, holding Data0 as well, cannot spare without spilling).
   constexpr bool PREFETCH = HEUN == 0;
-  // Stage 2 copies Data0 of update row J (= r-2 at iteration r) into shared memory two
-  // iterations ahead, without registers: one group per row, committed even when empty
+  // Stage 2 copies, without registers, the moments of row r+1 into shared memory while
+  // it works on row r, and Data0 of update row J+1 while it finishes row J (= r-2):
+  // one group per fetch, committed even when empty, so that the groups alternate
+  // U(r), D0(r-2), U(r+1), D0(r-1), ... and each wait leaves only the newest in flight
+  auto u_fetch = [&](int rr) {
+    if (HEUN == 1) {
+      if (col_in && rr >= 0 && rr < nyp) {
+        const long long idx = (long long)rr * pitch + C + 1;
+#pragma unroll
+        for (int n = 0; n < NV; n++) cp_async8(&win.Ua[n][lane], in + n * plane + idx);
+      }
+      cp_async_commit();
+    }
+  };
   auto d0_fetch = [&](int Jn) {
     if (HEUN == 1) {
       if (col_out && Jn >= NG && Jn <= nyp - 1 - NG && Jn >= w.J0 && Jn < w.J1) {
         const long long idx = (long long)Jn * pitch + C + 1;
 #pragma unroll
-        for (int n = 0; n < NV; n++) cp_async8(&win.D0[Jn & 1][n][lane], d0 + n * plane + idx);
+        for (int n = 0; n < NV; n++) cp_async8(&win.D0a[n][lane], d0 + n * plane + idx);
       }
       cp_async_commit();
     }
   };
+  u_fetch(rs);
   d0_fetch(rs - 2);
-  d0_fetch(rs - 1);
   double Un[NV];
   if (PREFETCH) {
     const bool ok = col_in && rs >= 0 && rs < nyp;
@@ -131,10 +144,15 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         const bool okn = col_in && r + 1 >= 0 && r + 1 < nyp;
         if (okn) load_cell(in, plane, (long long)(r + 1) * pitch + C + 1, Un);
         else benign(Un);
-      } else if (ok) {
-        load_cell(in, plane, (long long)r * pitch + C + 1, U);
       } else {
-        benign(U);
+        cp_async_wait_one();                 // this row's moments have landed
+        if (ok) {
+#pragma unroll
+          for (int n = 0; n < NV; n++) U[n] = win.Ua[n][lane];
+        } else {
+          benign(U);
+        }
+        u_fetch(r + 1);                      // into the slot just read
       }
       primitive(U, Q);
       if (ok && col_cell && r >= 1 && r <= nyp - 2) {
@@ -284,7 +302,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         if (HEUN == 1) {
           double R0[NV];
 #pragma unroll
-          for (int n = 0; n < NV; n++) U[n] = win.D0[J & 1][n][lane];
+          for (int n = 0; n < NV; n++) U[n] = win.D0a[n][lane];
           primitive(U, Q);
           relax<-1>(Q, R0, dt, Kn, Fx);
 #pragma unroll
@@ -307,7 +325,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
 #pragma unroll
       for (int n = 0; n < NV; n++) win.G[n][lane] = G[n];
     }
-    d0_fetch(r);                            // into the slot row J = r-2 has left
+    d0_fetch(r - 1);                        // the next update row, into the slot row J has left
     s0 = s0 == 2 ? 0 : s0 + 1;
   }
   if (HEUN == 1) cp_async_wait_all();       // nothing in flight past the work item
