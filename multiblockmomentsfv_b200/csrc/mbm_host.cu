@@ -94,7 +94,7 @@ struct mbm_ctx {
   int nwork = 0;
   std::vector<LimGroup> groups;
   int nsm = 0, ctas_per_sm = 1;
-  int seg_rows = 0;                 // rows per work item in use
+  double seg_rows = 0;              // rows per work item in use (ceil(rows / seg_rows) segments)
   CaseDev* dcase = nullptr;
   CaseDev* hcase = nullptr;         // pinned mirror, ncase entries
   unsigned long long* dlam = nullptr;
@@ -329,7 +329,7 @@ static int pitch_of(int nxp) { return (nxp + 1 + 3) & ~3; }
 
 // Work items grouped by limiter (the stage kernel is specialised per limiter):
 // blocks of cases with limiter L fill group L, strips within row segments.
-static void build_work(mbm_ctx* c, int seg_rows, std::vector<Work>& w) {
+static void build_work(mbm_ctx* c, double seg_rows, std::vector<Work>& w) {
   w.clear();
   c->groups.clear();
   for (int lim = 0; lim < 5; lim++) {
@@ -339,7 +339,7 @@ static void build_work(mbm_ctx* c, int seg_rows, std::vector<Work>& w) {
       const int nxp = c->hblk[b].nxp, nyp = c->hblk[b].nyp;
       const int nfx = nxp - 3, nfy = nyp - 3;          // face positions 1 .. nxp-3 / nyp-3
       const int strips = (nfx + STRIP - 1) / STRIP;
-      const int segs = std::max(1, (nfy + seg_rows - 1) / seg_rows);
+      const int segs = std::max(1, (int)std::ceil(nfy / seg_rows - 1e-9));
       for (int s = 0; s < segs; s++) {
         // equal-sized segments over face rows [1, nyp-3], the last one reaching nyp-2
         const int J0 = 1 + (int)((long long)nfy * s / segs);
@@ -349,7 +349,7 @@ static void build_work(mbm_ctx* c, int seg_rows, std::vector<Work>& w) {
     }
     const int count = (int)w.size() - start;
     if (count > 0) {
-      const int grid = (int)std::min<long long>((count + 3) / 4, (long long)c->nsm * c->ctas_per_sm);
+      const int grid = (int)std::min<long long>((count + CTA_WARPS - 1) / CTA_WARPS, (long long)c->nsm * c->ctas_per_sm);
       c->groups.push_back(LimGroup{lim, start, count, grid});
     }
   }
@@ -357,7 +357,17 @@ static void build_work(mbm_ctx* c, int seg_rows, std::vector<Work>& w) {
 
 // rebuild the work table for segments of `seg` rows; the table lives in the same
 // device buffer (sized for 8-row segments)
-static int set_segments(mbm_ctx* c, int seg) {
+// work items of a segment length (host only; the count build_work makes)
+static long long count_items(const mbm_ctx* c, double seg_rows) {
+  long long n = 0;
+  for (int b = 0; b < c->nblk; b++) {
+    const int nfx = c->hblk[b].nxp - 3, nfy = c->hblk[b].nyp - 3;
+    n += (long long)((nfx + STRIP - 1) / STRIP) * std::max(1, (int)std::ceil(nfy / seg_rows - 1e-9));
+  }
+  return n;
+}
+
+static int set_segments(mbm_ctx* c, double seg) {
   std::vector<Work> work;
   build_work(c, seg, work);
   c->nwork = (int)work.size();
@@ -431,7 +441,7 @@ static int push_cases(mbm_ctx* c) {
 // the fastest; the choice is cached per (strip rows, blocks, limiter mix, CTAs/SM)
 // for the life of the process.
 static std::mutex g_tune_mu;
-static std::map<std::tuple<long long, int, int, int>, int> g_tune_cache;
+static std::map<std::tuple<long long, int, int, int>, double> g_tune_cache;
 
 static int time_both_stages(mbm_ctx* c, cudaEvent_t e0, cudaEvent_t e1, float* ms) {
   for (int rep = 0; rep < 3; rep++) {
@@ -474,12 +484,29 @@ static int autotune(mbm_ctx* c) {
   LocalEvents ev;
   CK(cudaEventCreate(&ev.e[0]));
   CK(cudaEventCreate(&ev.e[1]));
-  int best = 32;
+  double best = 32;
   float best_ms = 1e30f;
-  // short segments buy parallelism on small grids, long ones save warm-up rows; every
-  // even length, because the last wave of the work queue makes the time jump with the
-  // item count (4 x 1024^2 cells: 22 rows 3.2 % faster than 24, 20 rows 5 % slower)
-  for (int seg = 8; seg <= 64; seg += 2) {
+  // short segments buy parallelism on small grids, long ones save warm-up rows.  The
+  // persistent grid's warps take the items from a queue, so the time jumps with the item
+  // count: besides every even length, each wave count k gets the shortest length whose
+  // items fill k waves of the resident warps without a partial one (the segment count is
+  // ceil(rows / length), so these lengths are fractional).  4 x 1024^2 cells: 22 rows
+  // (6,956 items, 3.92 waves) 3 % faster than 24, 20 rows 5 % slower, 21.4 rows (7,104
+  // items, 4 waves) 1.7 % faster than 22.
+  std::vector<double> cand;
+  for (int seg = 8; seg <= 64; seg += 2) cand.push_back(seg);
+  const long long W = (long long)c->nsm * c->ctas_per_sm * CTA_WARPS;
+  const long long most = count_items(c, 8.0), least = count_items(c, 64.0);
+  for (long long k = (least + W - 1) / W; k * W < most && k <= 64; k++) {
+    double lo = 8.0, hi = 64.0;              // count_items(hi) <= k W < count_items(lo)
+    for (int it = 0; it < 40; it++) {
+      const double mid = 0.5 * (lo + hi);
+      if (count_items(c, mid) <= k * W) hi = mid;
+      else lo = mid;
+    }
+    cand.push_back(hi);
+  }
+  for (double seg : cand) {
     st = set_segments(c, seg);
     float ms = 0.f;
     if (!st) st = time_both_stages(c, ev.e[0], ev.e[1], &ms);
@@ -1068,7 +1095,7 @@ extern "C" int mbm_config(mbm_ctx* c, int* segment_rows, int* work_items, int* c
   if (!c) return fail(c, MBM_EINVAL, "mbm_config: null context");
   int g = 0;
   for (const LimGroup& x : c->groups) g = std::max(g, x.grid);
-  if (segment_rows) *segment_rows = c->seg_rows;
+  if (segment_rows) *segment_rows = (int)std::lround(c->seg_rows);
   if (work_items) *work_items = c->nwork;
   if (ctas) *ctas = g;
   return MBM_OK;

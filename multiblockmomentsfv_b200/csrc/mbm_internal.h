@@ -19,6 +19,7 @@ namespace mbm {
 constexpr int NV = 9;           // moments per cell (src/defs.h:11)
 constexpr int NG = 3;           // ghost layers per edge (src/defs.h:14)
 constexpr int STRIP = 28;        // output columns per warp strip (32 lanes - 2 - 2 halo)
+constexpr int CTA_WARPS = 4;     // warps per CTA of the persistent stage kernel
 constexpr int MAX_TRACE = 4096;  // progress records kept per case and Steps call
 
 enum LayerSel : int { SEL_CUR = 0, SEL_OTHER = 1, SEL_TMP = 2 };

@@ -59,7 +59,7 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-constexpr int STAGE_WARPS = 4;
+constexpr int STAGE_WARPS = CTA_WARPS;
 #ifndef STAGE_MIN_CTAS
 #define STAGE_MIN_CTAS 3   // CTAs per SM the register budget is sized for (168 registers)
 #endif
