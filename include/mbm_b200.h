@@ -239,8 +239,9 @@ int mbm_shard_control(mbm_ctx *ctx, int *done);       /* accept/reject with the 
 int mbm_shard_end(mbm_ctx *ctx, double *t, int *nsteps, int *nrej);
 
 /* Launch configuration in use: rows per warp work item (picked by the autotuner
- * when mbm_params.segment_rows is 0), work items per stage, CTAs of the persistent
- * stage grid. */
+ * when mbm_params.segment_rows is 0; the tuner's length may be fractional -- a strip
+ * of n face rows gets ceil(n / length) equal segments -- and is reported rounded),
+ * work items per stage, CTAs of the persistent stage grid. */
 int mbm_config(mbm_ctx *ctx, int *segment_rows, int *work_items, int *ctas);
 
 /* Host-only: the resolved ghost-cell sources of a block table, 4 ints per ghost
