@@ -7,7 +7,8 @@
 // Iteration r loads the moments of row r, forms its projected primitives (raw
 // Primitive on the outermost ring, relaxed otherwise) into a three-row window in
 // shared memory, the y slopes of row r-1 and the y-face flux between rows r-2 and
-// r-1, then the x slopes and x-face states of row r-2 through warp shuffles, its
+// r-1, then the x slopes and x-face states of row r-2 (the left neighbour from the
+// window, the right-hand difference and face state through warp shuffles), its
 // x-face fluxes and its update.  Warps are independent (no barrier); a persistent
 // grid takes work items (block, strip, segment) from an atomic counter.  Every
 // cell's update keeps the reference's accumulation order
