@@ -88,10 +88,16 @@ def load_restart(deck: bf.Deck, path: str, faithful: bool = False):
 
 def main(argv=None) -> int:
     argv = sys.argv if argv is None else argv
+    if "-h" in argv[1:] or "--help" in argv[1:]:
+        print(__doc__)
+        return 0
     out_dir = _arg(argv, "-out", "")
     refine = _arg(argv, "-refine")
-    deck = bf.parse_file(_arg(argv, "-bfile", "blockfile.txt"),
-                         refine=max(1, int(float(refine))) if refine is not None else None)
+    bfile = _arg(argv, "-bfile", "blockfile.txt")
+    if not bfile or not os.path.isfile(bfile):
+        print("block file not found: %s (-h for the flags)" % bfile, file=sys.stderr)
+        return 1
+    deck = bf.parse_file(bfile, refine=max(1, int(float(refine))) if refine is not None else None)
     deck = deck.with_cli(Kn=_arg(argv, "-Kn"), R13=_arg(argv, "-R13"), CFL=_arg(argv, "-CFL"),
                          limiter=_arg(argv, "-limiter"))
     scn = _scenario(_arg(argv, "-scenario", "riemann2d"))

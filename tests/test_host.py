@@ -125,3 +125,13 @@ def test_scenario_matches_oracle_state(oracle_mod):
             oracle_mod.lib().orc_initial_state(C.byref(oracle_mod.c_scenario(s)), x, y, 0.0,
                                                U.ctypes.data_as(C.POINTER(C.c_double)))
             assert np.array_equal(U, sc.initial_state(s, x, y))
+
+
+def test_cli_help_and_missing_block_file(capsys):
+    """The command line answers -h with its flags and a missing block file with one
+    line on stderr and status 1 (no GPU needed for either)."""
+    from multiblockmomentsfv_b200 import __main__ as cli
+    assert cli.main(["prog", "-h"]) == 0
+    assert "-bfile" in capsys.readouterr().out
+    assert cli.main(["prog", "-bfile", "no/such/deck.txt"]) == 1
+    assert "block file not found" in capsys.readouterr().err
