@@ -264,17 +264,22 @@ int mbm_ghost_map(const mbm_block_desc *blocks, int nblocks, int *entries, int c
  * (DATA with filled ghosts); stage 2 (heun 1) reads `in` (TMP) and `data0` (DATA).
  * Interior cells of `out` are written; its ghost cells are left as they are (fill
  * them with SetBoundary semantics before the next stage).  Sync codes are ignored
- * here.  cfl[b] (host, may be NULL) receives each block's Update return value.
- * Launches on `stream` (a cudaStream_t, NULL = the legacy default stream) and
- * waits for it.
+ * here.  out must share no element with in or data0 (an in-place stage is
+ * refused with MBM_EINVAL: the kernel reads neighbours that other warps would have
+ * overwritten).  dt must be positive and finite.  cfl[b] (host, may be NULL)
+ * receives each block's Update return value.  A stage that writes a NaN or an
+ * infinity into out returns MBM_ENONFINITE (out and cfl are still written; a NaN
+ * never enters the CFL maxima, so cfl alone does not show it).  Launches on
+ * `stream` (a cudaStream_t, NULL = the legacy default stream) and waits for that
+ * stream before it returns.
  *
  * Scratch: one file-scope device array of 320 KB (held by every GPU that loads
- * the library until the process exits): at most 64 blocks and 19,968 warp work
+ * the library until the process exits): at most 64 blocks and 20,064 warp work
  * items (28-column strips x 32-row segments, e.g. 16 blocks of 1024^2); larger
- * inputs return MBM_EINVAL.  Its device address is looked up on the first call on
- * each device -- make that first call before any stream capture.  Every call
- * shares the array and clears what must start at zero; calls that overlap on the
- * GPU race.  Errors: mbm_last_error(NULL). */
+ * inputs return MBM_EINVAL.  Its device address is looked up by the first call on
+ * each device, with that device current -- make that first call before any stream
+ * capture.  Every call shares the array and clears what must start at zero; calls
+ * that overlap on the GPU race.  Errors: mbm_last_error(NULL). */
 int mbm_stage_noalloc(const mbm_block_desc *blocks, int nblocks, const double *in,
                       const double *data0, double *out, double Kn, double F, int limiter,
                       double dt, int heun, double *cfl, void *stream);

@@ -15,12 +15,17 @@
 // with cudaGetSymbolAddress, once per device, with that device current, on the
 // first call made on that device; that first call should therefore come before any
 // stream capture begins.  All calls share the array and it keeps the last call's
-// contents: each call clears the parts that must start at zero (the work counter
-// and the CFL maxima).  Two calls that overlap on the GPU (on different streams,
-// or from different host threads) race on the array.
+// contents: each call clears the parts that must start at zero (the work counter,
+// the CFL maxima and the non-finite flag).  Two calls that overlap on the GPU (on
+// different streams, or from different host threads) race on the array.  Each call
+// waits for its stream before it returns (it reads the CFL maxima and the
+// non-finite flag back to the host).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -52,6 +57,9 @@ constexpr int NOALLOC_MAX_WORK = (int)((NOALLOC_SCRATCH_BYTES - OFF_WORK) / size
 constexpr int NOALLOC_SEGMENT_ROWS = 32;
 
 static_assert(sizeof(CaseDev) <= OFF_QUEUE - OFF_CASE, "controller slot too small");
+// the capacity the header and the error message state; a layout change must update them
+static_assert(NOALLOC_MAX_WORK == 20064, "work-item capacity differs from the documented 20,064");
+static_assert(NOALLOC_MAX_BLOCKS == 64, "block capacity differs from the documented 64");
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
@@ -62,10 +70,17 @@ thread_local Work h_work[NOALLOC_MAX_WORK];
 thread_local BlockDev h_blk[NOALLOC_MAX_BLOCKS];
 thread_local unsigned long long h_lam[6 * NOALLOC_MAX_BLOCKS];
 thread_local CaseDev h_case;
+thread_local int h_nonfinite;
 
-int fail(int code, const char* msg) {
+int fail(int code, const std::string& msg) {
   set_global_error(msg);
   return code;
+}
+
+// [p, p + n doubles) and [q, q + n doubles) share an element
+bool overlaps(const double* p, const double* q, long long n) {
+  const uintptr_t a = (uintptr_t)p, b = (uintptr_t)q, len = (uintptr_t)n * sizeof(double);
+  return a < b + len && b < a + len;
 }
 
 }  // namespace
@@ -75,12 +90,11 @@ extern "C" int mbm_stage_noalloc(const mbm_block_desc* blocks, int nblocks, cons
                                  double dt, int heun, double* cfl, void* stream) {
   if (!blocks || nblocks < 1 || !in || !out || (heun == 1 && !data0) || (heun != 0 && heun != 1))
     return fail(MBM_EINVAL, "mbm_stage_noalloc: bad argument");
-  if (nblocks > NOALLOC_MAX_BLOCKS) return fail(MBM_EINVAL, "mbm_stage_noalloc: more than 64 blocks");
-  if (limiter < 0 || limiter > 4 || !(Kn > 1e-100 && Kn < 1e100) || !(dt > 0))
-    return fail(MBM_EINVAL, "mbm_stage_noalloc: bad limiter, Kn or dt");
+  if (nblocks > NOALLOC_MAX_BLOCKS)
+    return fail(MBM_EINVAL, "mbm_stage_noalloc: more than " + std::to_string(NOALLOC_MAX_BLOCKS) + " blocks");
+  if (limiter < 0 || limiter > 4 || !(Kn > 1e-100 && Kn < 1e100) || !(dt > 0) || !std::isfinite(dt))
+    return fail(MBM_EINVAL, "mbm_stage_noalloc: bad limiter, Kn or dt (dt must be positive and finite)");
   cudaStream_t s = (cudaStream_t)stream;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return fail(MBM_ENODEV, "no CUDA device");
 
   // block table in the layout of include/mbm_b200.h, and the warp work items
   long long off = 0;
@@ -104,14 +118,22 @@ extern "C" int mbm_stage_noalloc(const mbm_block_desc* blocks, int nblocks, cons
     const int strips = (nfx + STRIP - 1) / STRIP;
     const int segs = (nfy + NOALLOC_SEGMENT_ROWS - 1) / NOALLOC_SEGMENT_ROWS;
     if (nwork + (long long)strips * segs > NOALLOC_MAX_WORK)
-      return fail(MBM_EINVAL, "mbm_stage_noalloc: blocks exceed the scratch limit (19,968 warp work items: "
-                              "28-column strips x 32-row segments)");
+      return fail(MBM_EINVAL, "mbm_stage_noalloc: blocks exceed the scratch limit (" +
+                                  std::to_string(NOALLOC_MAX_WORK) + " warp work items: " +
+                                  std::to_string(STRIP) + "-column strips x " +
+                                  std::to_string(NOALLOC_SEGMENT_ROWS) + "-row segments)");
     for (int sg = 0; sg < segs; sg++) {
       const int J0 = 1 + (int)((long long)nfy * sg / segs);
       const int J1 = 1 + (int)((long long)nfy * (sg + 1) / segs);
       for (int k = 0; k < strips; k++) h_work[nwork++] = Work{b, 1 + STRIP * k, J0, J1};
     }
   }
+  // the kernel reads in (and data0) while other warps write out: out must share no
+  // element with either (an in-place stage would read cells already overwritten)
+  if (overlaps(out, in, off) || (heun == 1 && overlaps(out, data0, off)))
+    return fail(MBM_EINVAL, "mbm_stage_noalloc: out overlaps in or data0 (an in-place stage is not allowed)");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return fail(MBM_ENODEV, "no CUDA device");
   memset(&h_case, 0, sizeof h_case);
   h_case.dt = dt;
   h_case.Kn = Kn;
@@ -166,6 +188,8 @@ extern "C" int mbm_stage_noalloc(const mbm_block_desc* blocks, int nblocks, cons
   const long long grid = std::min<long long>((nwork + 3) / 4, (long long)sm * bitwise::stage_ctas_per_sm());
   e = bitwise::launch_stage(limiter, a, (int)grid, s);
   if (!e) e = cudaMemcpyAsync(h_lam, dlam, sizeof(unsigned long long) * 6 * nblocks, cudaMemcpyDeviceToHost, s);
+  if (!e) e = cudaMemcpyAsync(&h_nonfinite, (const unsigned char*)dcase + offsetof(CaseDev, nonfinite), sizeof(int),
+                              cudaMemcpyDeviceToHost, s);
   if (!e) e = cudaStreamSynchronize(s);
   if (e) return fail(MBM_ECUDA, cudaGetErrorString(e));
   if (cfl) {
@@ -175,5 +199,9 @@ extern "C" int mbm_stage_noalloc(const mbm_block_desc* blocks, int nblocks, cons
       cfl[b] = dt * v[0] / h_blk[b].dx + dt * v[1] / h_blk[b].dy + v[2];
     }
   }
+  // a NaN or infinity written to out: a NaN never enters the maxima above, so the CFL
+  // values alone would not show it
+  if (h_nonfinite)
+    return fail(MBM_ENONFINITE, "mbm_stage_noalloc: the stage wrote a NaN or infinity");
   return MBM_OK;
 }

@@ -25,7 +25,9 @@ from multiblockmomentsfv_b200 import output as out            # noqa: E402
 
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
-REF_SRC = "/root/reference/src"
+# the reference checkout (only read when the reference build is made here)
+REF_ROOT = os.environ.get("MBM_REFERENCE_ROOT", "/root/reference")
+REF_SRC = os.path.join(REF_ROOT, "src")
 
 NV, NG = 9, 3
 DATA, TMP, NEW = 0, 1, 2

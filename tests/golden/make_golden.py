@@ -40,7 +40,7 @@ def pack(zones, keep):
     )
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str = os.environ.get("MBM_REFERENCE_ROOT", "/root/reference")) -> None:
     os.makedirs(os.path.join(HERE, "decks"), exist_ok=True)
     for f in sorted(os.listdir(os.path.join(ref_root, "cases"))):
         shutil.copyfile(os.path.join(ref_root, "cases", f), os.path.join(HERE, "decks", f))

@@ -35,6 +35,55 @@ def test_create_without_device_fails_loudly():
     assert e.value.status == _abi.MBM_ENODEV
 
 
+def test_stage_noalloc_argument_checks():
+    """mbm_stage_noalloc refuses, before any CUDA call, an output that overlaps its
+    input or Data0 (an in-place stage), a non-finite or non-positive dt, too many
+    blocks and blocks beyond its scratch; the pointers are never dereferenced, so
+    plain integers stand in for device addresses."""
+    L = _abi.lib()
+    d = H.quadrant_deck(40, Kn=0.01, limiter=4)
+    descs = _abi.block_descs(d.blocks)
+    n = len(d.blocks)
+    total = 0
+    for b in d.blocks:      # the plane layout's element count (include/mbm_b200.h)
+        pitch = (b.nx + 6 + 1 + 3) // 4 * 4
+        total += 9 * ((pitch * (b.ny + 6) + 31) // 32 * 32)
+    base, nbytes = 1 << 40, total * 8
+    in_, d0 = base, base + 4 * nbytes
+
+    def call(inp, data0, out, dt=1e-3, heun=1, blocks=descs, nb=n):
+        st = L.mbm_stage_noalloc(blocks, nb, inp, data0, out, 0.01, 0.0, 4, dt, heun, None, None)
+        return st, L.mbm_last_error(None).decode()
+
+    for out_ in (in_, in_ + 8, in_ + nbytes - 8, in_ - nbytes + 8):
+        st, msg = call(in_, d0, out_)
+        assert st == _abi.MBM_EINVAL and "overlaps" in msg, (out_ - in_, msg)
+    for out_ in (d0, d0 + nbytes // 2, d0 - nbytes + 8):
+        st, msg = call(in_, d0, out_)
+        assert st == _abi.MBM_EINVAL and "overlaps" in msg, (out_ - d0, msg)
+    st, msg = call(in_, None, in_ + 8, heun=0)
+    assert st == _abi.MBM_EINVAL and "overlaps" in msg
+    for dt in (float("inf"), float("nan"), 0.0, -1e-3):
+        st, msg = call(in_, d0, base + 2 * nbytes, dt=dt)
+        assert st == _abi.MBM_EINVAL and "dt" in msg, dt
+    many = _abi.block_descs([d.blocks[0]] * 65)
+    st, msg = call(in_, d0, base + 2 * nbytes, blocks=many, nb=65)
+    assert st == _abi.MBM_EINVAL and "more than 64 blocks" in msg
+    big = _abi.block_descs([bf.Block(1, 0.0, 1.0, 0.0, 1.0, 8192, 8192, (0, 0, 0, 0))])
+    st, msg = call(in_, d0, base + 2 * nbytes, blocks=big, nb=1)
+    assert st == _abi.MBM_EINVAL and "scratch limit (20064 warp work items" in msg
+    # disjoint buffers pass every argument check: on a machine without a GPU the call
+    # then stops at the device lookup
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except ImportError:
+        has_gpu = False
+    if not has_gpu:
+        st, msg = call(in_, d0, base + 2 * nbytes)
+        assert st == _abi.MBM_ENODEV, msg
+
+
 @pytest.mark.parametrize("name", ["squareSmall", "square4", "square4Box", "Lshape", "ffs", "ffs28",
                                   "square16Uniform"])
 def test_ghost_map_equals_two_sweep_fill(oracle_mod, name):

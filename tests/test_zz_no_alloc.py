@@ -111,3 +111,30 @@ def test_stage_noalloc_rejects_oversize():
                              1e-4, 0, None, None)
     assert st == _abi.MBM_EINVAL
     assert b"scratch limit" in L.mbm_last_error(None)
+
+
+def test_stage_noalloc_reports_nonfinite():
+    """A NaN in one input cell makes the stage write NaNs; the call says so with
+    MBM_ENONFINITE (a NaN never enters the CFL maxima, so the CFL values alone would
+    not show it), and the next call on a finite input is MBM_OK again, because each
+    call clears the flag in the shared scratch."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    rng = np.random.default_rng(7)
+    d = H.quadrant_deck(24, Kn=0.01, limiter=4)
+    data = [H.random_layer(rng, b) for b in d.blocks]
+    L = _abi.lib()
+    descs = _abi.block_descs(d.blocks)
+    offs, total = plane_layout(d.blocks)
+    stream = torch.cuda.current_stream().cuda_stream
+    good = torch.from_numpy(to_planes(data, offs, total)).cuda()
+    data[1][10, 12, 3] = float("nan")
+    bad = torch.from_numpy(to_planes(data, offs, total)).cuda()
+    out = torch.zeros(total, dtype=torch.float64, device="cuda")
+    cfl = np.zeros(len(d.blocks))
+    for inp, want in ((bad, _abi.MBM_ENONFINITE), (good, _abi.MBM_OK), (bad, _abi.MBM_ENONFINITE)):
+        st = L.mbm_stage_noalloc(descs, len(d.blocks), inp.data_ptr(), None, out.data_ptr(), d.Kn, d.F,
+                                 d.limiter, 1e-3, 0, cfl.ctypes.data_as(C.POINTER(C.c_double)), stream)
+        assert st == want, (st, L.mbm_last_error(None))
+        assert np.isfinite(cfl).all()
