@@ -8,7 +8,7 @@
 Flags keep the reference's meaning and its quirks: numeric overrides pass through
 ``float`` (src/tools.c:38-46), -refine precedes the block file, and -sfile reloads the
 first zones of a result pair into L_DATA with the reference's mapping of the stored
-fields (src/Mesh.c:391-476: the stored pressure p goes where the temperature belongs and
+fields (src/Mesh.c:198-283: the stored pressure p goes where the temperature belongs and
 P_ij where T_ij belongs; -restart-faithful reads the last level with the correct
 mapping instead).  -scenario picks the initial/Dirichlet state that the
 reference hard-codes in src/Scenario.c (default riemann2d).  -fast runs the stage
@@ -46,7 +46,7 @@ def _scenario(spec: str) -> sc.Scenario:
 
 
 def load_restart(deck: bf.Deck, path: str, faithful: bool = False):
-    """LoadData (src/Mesh.c:391-476): the first len(blocks) zones fill the interior
+    """LoadData (src/Mesh.c:198-283): the first len(blocks) zones fill the interior
     plus one ghost ring of L_DATA; the remaining cells stay zero.  Like the reference,
     the stored pressure goes where the temperature belongs and P_ij where T_ij belongs,
     and the first zones of a multi-level file are its t = 0 level.

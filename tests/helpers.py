@@ -126,3 +126,25 @@ def random_deck(rng: np.random.Generator, max_n: int = 12) -> bf.Deck:
 
 
 quadrant_deck = bf.quadrant_deck
+
+# The reference's own regression tool (tools/compare_solution.py) and golden result
+# files, staged into oracle/_ref by `make -C oracle check` (part of the reference build).
+REF_BUILD = os.path.normpath(os.path.join(HERE, "..", "oracle", "_ref"))
+REF_COMPARE = os.path.join(REF_BUILD, "compare_solution.py")
+
+
+def reference_compare(new: str, ref: str, abstol=None, reltol=None):
+    """Run the reference's compare_solution.py on two .hdr/.dat results, as its
+    `make check` does; returns (passed, its stdout).  Skips the calling test when the
+    tool is not staged."""
+    import subprocess
+    import sys
+    import pytest
+    if not os.path.exists(REF_COMPARE):
+        pytest.skip("reference regression tool not staged (make -C oracle check)")
+    args = [sys.executable, REF_COMPARE, new, ref]
+    if abstol is not None:
+        args += [repr(float(abstol)), repr(float(reltol))]
+    r = subprocess.run(args, capture_output=True, text=True, timeout=1800)
+    assert r.returncode in (0, 1), r.stdout + r.stderr
+    return r.returncode == 0, r.stdout

@@ -146,6 +146,61 @@ def test_adjoint_against_oracle_differences(oracle_mod):
         assert abs(fd - ad) <= 1e-6 * abs(fd), (fd, ad)
 
 
+def _reference_replay(O, d, layers, dts):
+    """J after frozen-dt steps of the reference itself (its TimeUpdate from
+    oracle/_ref/libmbmref.so, then NEW -> DATA as its Steps copies, src/Main.c:236-240)."""
+    R = O.Reference(d)
+    for b, U in enumerate(layers):
+        R.set_layer(O.DATA, b, U)
+    R.set_boundary(O.DATA, 0.0)
+    t = 0.0
+    for dt in dts:
+        R.time_update(dt, t)
+        for b in range(len(d.blocks)):
+            R.set_layer(O.DATA, b, R.get_layer(O.NEW, b))
+        t += dt
+    J = 0.0
+    final = [R.get_layer(O.DATA, b) for b in range(len(d.blocks))]
+    for U in final:
+        P = output.primitive(U[bf.NG:-bf.NG, bf.NG:-bf.NG])
+        J += float(np.sum(P[..., 7] ** 2 + P[..., 8] ** 2))
+    return J, final
+
+
+def test_adjoint_against_reference_differences(oracle_mod):
+    """Directional derivatives from perturbed runs of the reference's own TimeUpdate
+    (the reference sources compiled into oracle/_ref), with the adjoint's frozen dt
+    sequence: the reference's unperturbed states equal the device replay bit for bit,
+    and its central differences (eps = 1e-6) match the adjoint to 1e-6."""
+    O = oracle_mod
+    if O.ref_lib() is None:
+        pytest.skip("reference build absent (make -C oracle ref)")
+    d = H.quadrant_deck(16, Kn=0.01, limiter=bf.LIM_AVERAGE)
+    base = adj.smooth_base(d, 5)
+    rng = np.random.default_rng(5)
+    th0 = _theta0(d, rng)
+    eps = 1e-6
+    with adj.Sensitivity(d, base) as S:
+        layers = adj.state_from_theta(d, base, th0)
+        S.load(layers)
+        J, g, gK, dts, ms = S.run(8, 3)
+        gth = adj.theta_gradient(d, layers, g)
+        S.load(layers)
+        S.replay(dts)
+        dev = [S.s.download(sv.L_DATA, b) for b in range(len(d.blocks))]
+    Jr, final = _reference_replay(O, d, layers, dts)
+    for b in range(len(d.blocks)):
+        H.assert_bitwise(dev[b][bf.NG:-bf.NG, bf.NG:-bf.NG], final[b][bf.NG:-bf.NG, bf.NG:-bf.NG], f"block {b + 1}")
+    assert abs(Jr - J) <= 1e-13 * abs(J)
+    for _ in range(4):
+        v = [rng.standard_normal(t.shape) for t in th0]
+        Jp, _ = _reference_replay(O, d, adj.state_from_theta(d, base, [t + eps * w for t, w in zip(th0, v)]), dts)
+        Jm, _ = _reference_replay(O, d, adj.state_from_theta(d, base, [t - eps * w for t, w in zip(th0, v)]), dts)
+        fd = (Jp - Jm) / (2 * eps)
+        ad = sum(float(np.sum(a * w)) for a, w in zip(gth, v))
+        assert abs(fd - ad) <= 1e-6 * abs(fd), (fd, ad)
+
+
 def test_autograd_function():
     torch = pytest.importorskip("torch")
     d = H.quadrant_deck(16, Kn=0.01)

@@ -136,7 +136,8 @@ def test_fast_end_time_benchmark():
 def test_fast_reference_deck_regression_gate(tmp_path):
     """cases/squareSmall.txt (Riemann2D, 7 output levels to t = 0.3) written with
     -double in both modes; the reference's regression comparison at its Float64
-    defaults passes."""
+    defaults passes, restated (output.compare) and run as the reference's own
+    tools/compare_solution.py."""
     d = H.deck("squareSmall")
     scn = sc.Scenario.named("riemann2d")
     w_ref, n_ref = sv.run(d, scn, str(tmp_path / "exact"), single=False, verbose=False, mode="exact")
@@ -144,6 +145,8 @@ def test_fast_reference_deck_regression_gate(tmp_path):
     assert n_ref == n_fast
     ok, mx, msg = output.compare(w_fast.base, w_ref.base)
     assert ok, msg
+    ok, log = H.reference_compare(w_fast.base, w_ref.base)   # the reference's own tool
+    assert ok and log.startswith("PASS"), log
 
 
 def test_fast_batch_equals_fast_alone():

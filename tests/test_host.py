@@ -184,3 +184,42 @@ def test_cli_help_and_missing_block_file(capsys):
     assert "-bfile" in capsys.readouterr().out
     assert cli.main(["prog", "-bfile", "no/such/deck.txt"]) == 1
     assert "block file not found" in capsys.readouterr().err
+
+
+@pytest.mark.parametrize("single", [False, True])
+def test_regression_gate_equals_reference_tool(tmp_path, single):
+    """output.compare, the package's restatement of the reference's regression gate,
+    against the reference's own tools/compare_solution.py (staged by the reference
+    build) on result files differing by planted amounts around the gate's threshold,
+    at the default tolerances and at zero tolerance."""
+    rng = np.random.default_rng(11 + single)
+    d = H.quadrant_deck(12, Kn=0.01, limiter=4)
+    layers = [H.random_layer(rng, b) for b in d.blocks]
+    base = out.Writer(str(tmp_path / "base"), d, "Riemann2D", single=single)
+    base.write(layers, 0.0, 0)
+    base.write(layers, 0.1, 1)
+    abstol, reltol = (1e-6, 1e-5) if single else (1e-10, 1e-8)
+    cases = [0.0, 0.5, 0.9, 1.1, 3.0]       # planted difference / threshold at one value
+    seen = set()
+    for k, f in enumerate(cases):
+        w = out.Writer(str(tmp_path / f"c{k}"), d, "Riemann2D", single=single)
+        w.write(layers, 0.0, 0)
+        w.write(layers, 0.1, 1)
+        # plant the difference in one value of the second level's first zone
+        _, dat = out.companion(w.base)
+        esize = 4 if single else 8
+        z = out.read(w.base)[0][len(d.blocks)]
+        idx = 37
+        y = float(z["values"].ravel()[idx])
+        x = np.array([y + f * (abstol + reltol * abs(y))], dtype="<f4" if single else "<f8")
+        raw = bytearray(open(dat, "rb").read())
+        raw[z["offset"] + idx * esize: z["offset"] + (idx + 1) * esize] = x.tobytes()
+        open(dat, "wb").write(bytes(raw))
+        ok_pkg, _, msg = out.compare(w.base, base.base)
+        ok_ref, log = H.reference_compare(w.base, base.base)
+        assert ok_pkg == ok_ref, (f, msg, log)
+        seen.add(ok_ref)
+        ok0_pkg = out.compare(w.base, base.base, 0.0, 0.0)[0]
+        ok0_ref = H.reference_compare(w.base, base.base, 0.0, 0.0)[0]
+        assert ok0_pkg == ok0_ref == (f == 0.0), f
+    assert seen == {True, False}

@@ -56,6 +56,29 @@ def test_square4_golden_bitwise(oracle_mod, tmp_path):
     assert np.array_equal(vals.view(np.uint32), g["values"].view(np.uint32))
 
 
+def test_squareSmall_reference_check(oracle_mod, tmp_path):
+    """The reference's `make check` comparison on the CPU side: the oracle's run of
+    cases/squareSmall.txt and the unmodified reference binary's both pass the
+    reference's tools/compare_solution.py against reference/squareSmall.ref."""
+    golden = os.path.join(H.REF_BUILD, "squareSmall.ref")
+    if not os.path.exists(golden + ".hdr"):
+        pytest.skip("reference goldens not staged (make -C oracle check)")
+    d = H.deck("squareSmall")
+    w, _ = oracle_mod.run_deck(d, sc.Scenario.named("riemann2d"), str(tmp_path / "oracle"))
+    ok, log = H.reference_compare(w.hdr, golden, 0.0, 0.0)
+    assert ok, log
+    exe = os.path.join(H.REF_BUILD, "moments")
+    if os.path.exists(exe):
+        import subprocess
+        env = dict(os.environ, MBM_SCENARIO="riemann2d", OMP_NUM_THREADS="1")
+        r = subprocess.run([exe, "-bfile", os.path.join(H.DECKS, "squareSmall.txt"), "-out", str(tmp_path / "ref")],
+                           env=env, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout[-2000:]
+        hdr = [f for f in os.listdir(tmp_path / "ref") if f.endswith("_tAll.hdr")][0]
+        ok, log = H.reference_compare(str(tmp_path / "ref" / hdr), golden)
+        assert ok and log.startswith("PASS"), log
+
+
 def test_oracle_output_writer_matches_manifest(oracle_mod, tmp_path):
     d = H.deck("squareSmall", t_out=[0.05])
     w, n = oracle_mod.run_deck(d, sc.Scenario.named("riemann2d"), str(tmp_path))

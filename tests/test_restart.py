@@ -2,6 +2,7 @@
 opt-in faithful mapping (-restart-faithful) that reloads the last written level into
 the state it came from.  Host only."""
 import numpy as np
+import pytest
 
 import helpers as H
 from multiblockmomentsfv_b200 import __main__ as cli
@@ -54,3 +55,38 @@ def test_default_restart_keeps_the_references_mapping(tmp_path):
         assert np.allclose(a[..., 0], 2.0)
         assert np.allclose(a[..., 3], 1.5 * 2.0 * 2.0)      # theta taken as p = 2
         assert np.allclose(a[..., 4], 2.0 * 2.0)            # T11 taken as P11 = 2
+
+
+def _reference_load(d, path):
+    """The reference's own LoadData (src/Mesh.c:198-283, oracle/_ref/libmbmref.so)
+    into DB_Block layers whose L_DATA starts at zero, as main allocates it."""
+    import ctypes as C
+    import os
+    import sys
+    import pytest
+    sys.path.insert(0, os.path.join(H.HERE, "..", "oracle"))
+    import oracle as O
+    if O.ref_lib() is None:
+        pytest.skip("reference sources not built here")
+    ref = O.Reference(d)
+    O.ref_lib().LoadData.argtypes = [C.POINTER(O.DBBlock), C.c_int, C.c_char_p]
+    O.ref_lib().LoadData(ref.B, len(d.blocks), path.encode())
+    return [ref.get_layer(O.DATA, b) for b in range(len(d.blocks))]
+
+
+@pytest.mark.parametrize("single", [False, True])
+@pytest.mark.parametrize("deck", ["squareSmall", "Lshape"])
+def test_default_restart_equals_reference_loaddata(tmp_path, deck, single):
+    """The package's restart loader (default mapping) against the reference's own
+    LoadData on the same file: every cell of L_DATA bit for bit, on a two-level
+    result file (the first level is read) in both payload precisions."""
+    d = H.deck(deck)
+    lv = _levels(d, 3 + single)
+    w = output.Writer(str(tmp_path), d, "Riemann2D", single=single)
+    w.write(lv[0], 0.0, -1)
+    w.write(lv[1], 0.1, 5)
+    for name in (w.base, w.hdr, w.dat):        # basename, .hdr or .dat, as LoadData accepts
+        ref = _reference_load(d, name)
+        got = cli.load_restart(d, name)
+        for b in range(len(d.blocks)):
+            H.assert_bitwise(got[b], ref[b], f"{deck} block {b + 1} ({name[-4:]})")
