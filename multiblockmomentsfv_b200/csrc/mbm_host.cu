@@ -84,6 +84,7 @@ struct mbm_ctx {
   BlockDev* dblk = nullptr;
   long long layer_elems = 0;
   double* buf[3] = {nullptr, nullptr, nullptr};
+  double* rlx = nullptr;            // fast arithmetic: the stage-1 relaxation term (a layer)
   double* staging = nullptr;        // array-of-structs transfer buffer, one block
   GhostEntry* dghost = nullptr;
   int nghost = 0;
@@ -379,8 +380,11 @@ static int set_segments(mbm_ctx* c, double seg) {
 
 // one Heun stage of every block: one persistent launch per limiter group
 // (with several limiter groups, group k > 0 runs on aux stream k-1, so that one
-// group's CTAs fill the SMs another group's tail leaves idle)
-static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, int sel_out,
+// group's CTAs fill the SMs another group's tail leaves idle).  rlx_read (stage 2,
+// fast arithmetic): the relaxation term of Data0 is read from what the stage 1 of
+// the same attempt stored, instead of being formed again -- only where that stage 1
+// ran on the same Data0 just before.
+static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, int sel_out, int rlx_read,
                                  double* const* bufs = nullptr) {
   const int ng = (int)c->groups.size();
   cudaError_t e0;
@@ -402,6 +406,8 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
     a.queue = c->dqueue + heun * 5 + g.lim;
     a.sel_in = sel_in; a.sel_d0 = sel_d0; a.sel_out = sel_out;
     a.heun = heun;
+    a.rlx = c->rlx;
+    a.rlx_read = heun == 1 && rlx_read;
     cudaError_t e = c->fast ? fastmath::launch_stage(g.lim, a, g.grid, st)
                             : bitwise::launch_stage(g.lim, a, g.grid, st);
     if (e != cudaSuccess) return e;
@@ -416,9 +422,9 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
 // the body of one step attempt: stage 1, fill TMP, stage 2, fill NEW, controller
 static cudaError_t launch_attempt(mbm_ctx* c, cudaGraphConditionalHandle h, int use_handle) {
   cudaError_t e;
-  if ((e = launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP))) return e;
+  if ((e = launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP, 0))) return e;
   if ((e = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_TMP, c->stream))) return e;
-  if ((e = launch_stages(c, 1, SEL_TMP, SEL_CUR, SEL_OTHER))) return e;
+  if ((e = launch_stages(c, 1, SEL_TMP, SEL_CUR, SEL_OTHER, 1))) return e;
   if ((e = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_OTHER, c->stream))) return e;
   if ((e = launch_control(c->dcase, c->ncase, c->dblk, c->dlam, c->dtrace, c->dqueue, h, use_handle, c->stream)))
     return e;
@@ -448,7 +454,7 @@ static int time_both_stages(mbm_ctx* c, cudaEvent_t e0, cudaEvent_t e1, float* m
     if (rep == 1) CK(cudaEventRecord(e0, c->stream));
     for (int heun = 0; heun < 2; heun++) {
       CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
-      CK(launch_stages(c, heun, heun ? SEL_TMP : SEL_CUR, SEL_CUR, heun ? SEL_OTHER : SEL_TMP));
+      CK(launch_stages(c, heun, heun ? SEL_TMP : SEL_CUR, SEL_CUR, heun ? SEL_OTHER : SEL_TMP, 1));
     }
   }
   CK(cudaEventRecord(e1, c->stream));
@@ -596,6 +602,7 @@ static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vecto
   }
   if (c->prm.max_attempts <= 0) c->prm.max_attempts = 10000000;
   c->adjoint = params->adjoint != 0 && ncases == 1;
+  c->fast = params->mode == MBM_MODE_FAST;
   c->device = params->device;
   c->nblk = nblocks;
   c->ncase = ncases;
@@ -646,6 +653,10 @@ static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vecto
   for (int l = 0; l < 3; l++) {
     CKC(cudaMalloc(&c->buf[l], sizeof(double) * off));
     CKC(cudaMemsetAsync(c->buf[l], 0, sizeof(double) * off, c->stream));
+  }
+  if (c->fast) {
+    CKC(cudaMalloc(&c->rlx, sizeof(double) * off));
+    CKC(cudaMemsetAsync(c->rlx, 0, sizeof(double) * off, c->stream));
   }
   CKC(cudaMalloc(&c->staging, sizeof(double) * max_cells * (NV + 1)));   // layers, or 10 output fields
   CKC(cudaMalloc(&c->dblk, sizeof(BlockDev) * nblocks));
@@ -707,7 +718,6 @@ static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vecto
 
   // work table and grid
   CKC(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device));
-  c->fast = params->mode == MBM_MODE_FAST;
   c->ctas_per_sm = c->fast ? fastmath::stage_ctas_per_sm() : bitwise::stage_ctas_per_sm();
   long long max_items = 0;
   for (auto& d : c->hblk) max_items += (long long)((d.nxp - 3 + STRIP - 1) / STRIP) * ((d.nyp - 3 + 7) / 8 + 1);
@@ -792,6 +802,7 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
   for (int l = 0; l < 3; l++) cudaFree(c->buf[l]);
+  cudaFree(c->rlx);
   cudaFree(c->staging);
   cudaFree(c->dblk);
   cudaFree(c->dghost);
@@ -959,9 +970,10 @@ extern "C" int mbm_set_boundary(mbm_ctx* c, int layer, double t) {
   return wait_stream(c);
 }
 
-static int run_stage(mbm_ctx* c, int out_layer, int in_layer, int d0_layer, int heun, double* cfl) {
+static int run_stage(mbm_ctx* c, int out_layer, int in_layer, int d0_layer, int heun, double* cfl,
+                     int rlx_read = 0) {
   CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
-  CK(launch_stages(c, heun, layer_sel(in_layer), layer_sel(d0_layer), layer_sel(out_layer)));
+  CK(launch_stages(c, heun, layer_sel(in_layer), layer_sel(d0_layer), layer_sel(out_layer), rlx_read));
   CK(launch_stage_cfl(c->dblk, c->nblk, c->dcase, c->dlam, heun, c->dcfl, c->stream));
   CK(cudaMemcpyAsync(c->hcfl, c->dcfl, sizeof(double) * c->nblk, cudaMemcpyDeviceToHost, c->stream));
   int st = wait_stream(c);
@@ -992,7 +1004,7 @@ extern "C" int mbm_time_update(mbm_ctx* c, double dt, double t, double* cfl) {
   if (st) return st;
   for (double x : v) if (x > c1) c1 = x;
   if ((st = mbm_set_boundary(c, MBM_L_TMP, t + dt))) return st;
-  st = run_stage(c, MBM_L_NEW, MBM_L_TMP, MBM_L_DATA, 1, v.data());
+  st = run_stage(c, MBM_L_NEW, MBM_L_TMP, MBM_L_DATA, 1, v.data(), 1);   // stage 1 ran on DATA
   if (st) return st;
   for (double x : v) if (x > c2) c2 = x;
   if ((st = mbm_set_boundary(c, MBM_L_NEW, t + dt))) return st;
@@ -1134,12 +1146,12 @@ extern "C" int mbm_time_stage(mbm_ctx* c, int heun, double dt, int reps, double*
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
-  CK(launch_stages(c, heun, si, SEL_CUR, so));      // warm-up launch
+  CK(launch_stages(c, heun, si, SEL_CUR, so, 1));      // warm-up launch
   // the per-launch queue reset is a 40-byte memset, inside the timed region
   CK(cudaEventRecord(e0, c->stream));
   for (int r = 0; r < reps; r++) {
     CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
-    CK(launch_stages(c, heun, si, SEL_CUR, so));
+    CK(launch_stages(c, heun, si, SEL_CUR, so, 1));
   }
   CK(cudaEventRecord(e1, c->stream));
   CK(launch_stage_cfl(c->dblk, c->nblk, c->dcase, c->dlam, heun, c->dcfl, c->stream));
@@ -1251,10 +1263,10 @@ static int frozen_step(mbm_ctx* c, const double* in, double* out, const double* 
   double* bufs[3] = {const_cast<double*>(in), out, tmp};
   CK(cudaMemcpyAsync(&c->dcase[0].dt, ddt, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
-  CK(launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP, bufs));
+  CK(launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP, 0, bufs));
   CK(launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, bufs, c->ddir, SEL_TMP, c->stream));
   if (!out) return MBM_OK;
-  CK(launch_stages(c, 1, SEL_TMP, SEL_CUR, SEL_OTHER, bufs));
+  CK(launch_stages(c, 1, SEL_TMP, SEL_CUR, SEL_OTHER, 1, bufs));
   CK(launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, bufs, c->ddir, SEL_OTHER, c->stream));
   return MBM_OK;
 }
@@ -1672,7 +1684,7 @@ extern "C" int mbm_shard_stage(mbm_ctx* c, int heun) {
   if (heun != 0 && heun != 1) return fail(c, MBM_EINVAL, "mbm_shard_stage: bad argument");
   CK(cudaSetDevice(c->device));
   CK(cudaMemsetAsync(c->dqueue + heun * 5, 0, sizeof(int) * 5, c->stream));
-  CK(launch_stages(c, heun, heun ? SEL_TMP : SEL_CUR, SEL_CUR, heun ? SEL_OTHER : SEL_TMP));
+  CK(launch_stages(c, heun, heun ? SEL_TMP : SEL_CUR, SEL_CUR, heun ? SEL_OTHER : SEL_TMP, 1));
   return MBM_OK;
 }
 

@@ -71,6 +71,12 @@ struct StageArgs {
   int* queue;                // work-item counter of this stage (zero before the launch)
   int sel_in, sel_d0, sel_out;
   int heun;
+  // fast arithmetic only: the relaxation term of the stage-1 input (layer layout,
+  // interior cells), written by stage 1; rlx_read = 1 makes stage 2 read it in place
+  // of forming it again from Data0 (set only when the stage 1 of the same attempt,
+  // on the same Data0, ran just before)
+  double* rlx;
+  int rlx_read;
 };
 
 struct AdjArgs {       // one stage of the discrete adjoint (mbm_adjoint.cu)

@@ -340,6 +340,34 @@ __device__ __forceinline__ void relax_prim(const double (&P)[NV], double (&Q)[NV
 #endif
 
 #if MBM_FAST_ARITH
+// The damping factors of flags 0 (= -1) and 1 at z and 2z/3 (src/Flux.c:213-223) from
+// one reciprocal per argument (fast arithmetic): both share the denominator
+// 1 + z + z^2/4 = (1 + z/2)^2, so with w = 1/(1 + z/2)
+//   R_0(z) = (1 + z/2 - z^2/4) w^2,   R_1(z) = (1 + z) w^2.
+struct Damp01 {
+  double d1_0, d2_0;   // flag 0 / -1: R(z), R(2z/3)
+  double d1_1, d2_1;   // flag 1
+  __device__ __forceinline__ explicit Damp01(double z) {
+    const double z2 = 2.0 / 3 * z;
+    const double w1 = frcp(fma(0.5, z, 1.0)), w2 = frcp(fma(0.5, z2, 1.0));
+    const double s1 = w1 * w1, s2 = w2 * w2;
+    d1_0 = fma(z, fma(-0.25, z, 0.5), 1.0) * s1;
+    d2_0 = fma(z2, fma(-0.25, z2, 0.5), 1.0) * s2;
+    d1_1 = (1.0 + z) * s1;
+    d2_1 = (1.0 + z2) * s2;
+  }
+};
+
+// the moments of relax<-1>(P) (ProductionsDirect without the force, src/Flux.c:230-267)
+// given its damping factors d1 = R(z), d2 = R(2z/3) (fast arithmetic)
+__device__ __forceinline__ void relaxed_moments(const double (&P)[NV], double d1, double d2,
+                                                double (&Out)[NV]) {
+  const double rho = P[0], v1 = P[1], v2 = P[2], th = P[3];
+  const double E = rho * fma(0.5, fma(v1, v1, v2 * v2), 1.5 * th);
+  moments_e(rho, v1, v2, E, fma(d1, P[4] - th, th), d1 * P[5], fma(d1, P[6] - th, th), d2 * P[7], d2 * P[8],
+            Out);
+}
+
 // relax<2>(Primitive(U)) in moment form (fast arithmetic): flag 2 leaves T and q as
 // they are (R = 1), so only the push of the velocity by g = dt F changes the moments:
 //   U1 + rho g,  E + g (U1 + rho g/2),  U4 + g (2 U1 + rho g),  U5 + g U2,
@@ -357,6 +385,9 @@ __device__ __forceinline__ void push_moments(const double (&U)[NV], double g, do
   R[7] = fma(g, U[3] + U[4] + 0.5 * g * fma(3.0, U[1], rg), U[7]);
   R[8] = fma(g, fma(0.5 * g, U[2], U[5]), U[8]);
 }
+// The same push applies to any moment vector whose temperature and heat flux stay
+// fixed: relax<0>(P) = push_moments(relax<-1>(P), dt F), flag 0 differing from flag
+// -1 only by the force acting on the velocity before the moments are formed.
 #endif
 
 // only the CFL share of relax<FLAG> (same z, same factor)

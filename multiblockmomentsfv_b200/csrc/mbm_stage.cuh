@@ -77,6 +77,16 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   const double* __restrict__ in = a.buf[phys_layer(a.sel_in, cur)] + B.off;
   const double* __restrict__ d0 = a.buf[phys_layer(a.sel_d0, cur)] + B.off;
   double* __restrict__ out = a.buf[phys_layer(a.sel_out, cur)] + B.off;
+#if MBM_FAST_ARITH
+  // the relaxation term of the stage-1 input: written by stage 1 at its row r and read
+  // back (plain loads: written in this launch) by the update of that row two
+  // iterations later; stage 2 reads it with rlx_read in place of forming it from Data0
+  double* __restrict__ rlx = a.rlx + B.off;
+  const bool rlx_rd = HEUN == 1 && a.rlx_read;
+  const double* __restrict__ d0src = rlx_rd ? rlx : d0;
+#else
+  const double* __restrict__ d0src = d0;
+#endif
   const int nxp = B.nxp, nyp = B.nyp, pitch = B.pitch;
   const long long plane = B.plane;
   const int C = w.I0 - 2 + lane;
@@ -120,7 +130,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
       if (col_out && Jn >= NG && Jn <= nyp - 1 - NG && Jn >= w.J0 && Jn < w.J1) {
         const long long idx = (long long)Jn * pitch + C + 1;
 #pragma unroll
-        for (int n = 0; n < NV; n++) cp_async8(&win.D0a[n][lane], d0 + n * plane + idx);
+        for (int n = 0; n < NV; n++) cp_async8(&win.D0a[n][lane], d0src + n * plane + idx);
       }
       cp_async_commit();
     }
@@ -156,16 +166,45 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         u_fetch(r + 1);                      // into the slot just read
       }
       primitive(U, Q);
-      if (ok && col_cell && r >= 1 && r <= nyp - 2) {
+#if MBM_FAST_ARITH
+      if (HEUN == 0) {
+        // stage 1: one collision number and one reciprocal per damping argument serve
+        // the CFL share (flag 0), the relaxation term of the update (flag -1, stored for
+        // the update of this row and for stage 2) and the projection (flag 1)
+        const Damp01 dm(Q[0] * fsqrt(Q[3]) * Kn.r * dt);
+        if (ok && col_cell && r >= 1 && r <= nyp - 2) {
+          const double c = 0.5 * (1 - dm.d2_0);
+          if (c > prod) prod = c;
+        }
+        if (ok && col_out && r >= NG && r <= nyp - 1 - NG && r >= w.J0 && r < w.J1) {
+          double R0[NV];
+          relaxed_moments(Q, dm.d1_0, dm.d2_0, R0);
+          const long long idx = (long long)r * pitch + C + 1;
+#pragma unroll
+          for (int n = 0; n < NV; n++) rlx[n * plane + idx] = R0[n];
+        }
+        if (!(col_ring || r == 0 || r == nyp - 1)) {
+          const double th = Q[3];
+          Q[4] = fma(dm.d1_1, Q[4] - th, th);
+          Q[5] = dm.d1_1 * Q[5];
+          Q[6] = fma(dm.d1_1, Q[6] - th, th);
+          Q[7] = dm.d2_1 * Q[7];
+          Q[8] = dm.d2_1 * Q[8];
+        }
+      }
+#endif
+      if (!MBM_FAST_ARITH && ok && col_cell && r >= 1 && r <= nyp - 2) {
         const double c = relax_cfl<2 * HEUN>(Q, dt, Kn);
         if (c > prod) prod = c;
       }
       if (!(col_ring || r == 0 || r == nyp - 1)) {
 #if MBM_FAST_ARITH
-        double V[NV];
-        relax_prim<2 * HEUN + 1>(Q, V, dt, Kn, Fx);
+        if (HEUN == 1) {   // stage 2 (flag 3): no CFL share (flag 2 is the identity)
+          double V[NV];
+          relax_prim<3>(Q, V, dt, Kn, Fx);
 #pragma unroll
-        for (int n = 0; n < NV; n++) Q[n] = V[n];
+          for (int n = 0; n < NV; n++) Q[n] = V[n];
+        }
 #else
         double V[NV];
         relax<2 * HEUN + 1>(Q, V, dt, Kn, Fx);
@@ -288,15 +327,24 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
       if (col_out && J >= NG && J <= nyp - 1 - NG) {
         const long long idx = (long long)J * pitch + C + 1;
         double U[NV], Q[NV], R[NV];
-        load_cell(in, plane, idx, U);
 #if MBM_FAST_ARITH
+        const double g = dt * Fx;
         if (HEUN == 1) {
-          push_moments(U, dt * Fx, R);        // relax<2>: the force push alone
+          load_cell(in, plane, idx, U);
         } else {
-          primitive(U, Q);
-          relax<0>(Q, R, dt, Kn, Fx);
+#pragma unroll
+          for (int n = 0; n < NV; n++) U[n] = rlx[n * plane + idx];   // relax<-1> of this cell
+        }
+        // stage 1: relax<0> = the force push of relax<-1>; stage 2: relax<2> = the force
+        // push of the moments (both the identity without a force)
+        if (g != 0.0) {
+          push_moments(U, g, R);
+        } else {
+#pragma unroll
+          for (int n = 0; n < NV; n++) R[n] = U[n];
         }
 #else
+        load_cell(in, plane, idx, U);
         primitive(U, Q);
         relax<2 * HEUN>(Q, R, dt, Kn, Fx);
 #endif
@@ -304,8 +352,18 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
           double R0[NV];
 #pragma unroll
           for (int n = 0; n < NV; n++) U[n] = win.D0a[n][lane];
+#if MBM_FAST_ARITH
+          if (rlx_rd) {                       // relax<-1>(Data0), stored by stage 1
+#pragma unroll
+            for (int n = 0; n < NV; n++) R0[n] = U[n];
+          } else {
+            primitive(U, Q);
+            relax<-1>(Q, R0, dt, Kn, Fx);
+          }
+#else
           primitive(U, Q);
           relax<-1>(Q, R0, dt, Kn, Fx);
+#endif
 #pragma unroll
           for (int n = 0; n < NV; n++) R[n] += R0[n];
         }
