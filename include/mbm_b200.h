@@ -235,7 +235,12 @@ int mbm_shard_stage(mbm_ctx *ctx, int heun);          /* Heun stage 1 (DATA -> T
 int mbm_shard_pack(mbm_ctx *ctx, int layer);          /* this rank's cells other ranks need */
 int mbm_shard_fill(mbm_ctx *ctx, int layer);          /* SetBoundary of the layer, remote cells received */
 int mbm_shard_cfl(mbm_ctx *ctx);                      /* this rank's CFL of the attempt -> the scalar */
-int mbm_shard_control(mbm_ctx *ctx, int *done);       /* accept/reject with the scalar; waits */
+/* accept/reject with the scalar.  done non-NULL: waits for the stream and reports
+ * whether the step loop has finished; NULL: enqueues the controller and returns at
+ * once -- the stage, fill and controller kernels of a finished case return at once,
+ * so a caller may enqueue several attempts (every rank the same number) and read
+ * `done` once per batch. */
+int mbm_shard_control(mbm_ctx *ctx, int *done);
 int mbm_shard_end(mbm_ctx *ctx, double *t, int *nsteps, int *nrej);
 
 /* Launch configuration in use: rows per warp work item (picked by the autotuner

@@ -22,11 +22,13 @@
 namespace mbm {
 namespace bitwise {
 cudaError_t launch_stage(int lim, const StageArgs& a, int grid, cudaStream_t s);
-int stage_ctas_per_sm();
+int stage_ctas_per_sm(int heun);
+int stage_cta_warps();
 }
 namespace fastmath {
 cudaError_t launch_stage(int lim, const StageArgs& a, int grid, cudaStream_t s);
-int stage_ctas_per_sm();
+int stage_ctas_per_sm(int heun);
+int stage_cta_warps();
 }
 cudaError_t launch_ghost(const BlockDev* blk, const CaseDev* cases, const GhostEntry* map, int n,
                          double* const buf[3], const double* dirichlet, int sel, cudaStream_t s,
@@ -69,7 +71,8 @@ void set_global_error(const std::string& msg) { g_create_error = msg; }
 }  // namespace mbm
 
 struct LimGroup {      // the work items of every block whose case uses one limiter
-  int lim, start, count, grid;
+  int lim, start, count;
+  int grid[2];         // persistent grid of each Heun stage
 };
 
 struct mbm_ctx {
@@ -94,7 +97,8 @@ struct mbm_ctx {
   Work* dwork = nullptr;
   int nwork = 0;
   std::vector<LimGroup> groups;
-  int nsm = 0, ctas_per_sm = 1;
+  int nsm = 0, cta_warps = CTA_WARPS;   // stage kernel: warps per CTA
+  int ctas_per_sm[2] = {1, 1};          // stage kernel: resident CTAs per SM of each Heun stage
   double seg_rows = 0;              // rows per work item in use (ceil(rows / seg_rows) segments)
   CaseDev* dcase = nullptr;
   CaseDev* hcase = nullptr;         // pinned mirror, ncase entries
@@ -350,8 +354,11 @@ static void build_work(mbm_ctx* c, double seg_rows, std::vector<Work>& w) {
     }
     const int count = (int)w.size() - start;
     if (count > 0) {
-      const int grid = (int)std::min<long long>((count + CTA_WARPS - 1) / CTA_WARPS, (long long)c->nsm * c->ctas_per_sm);
-      c->groups.push_back(LimGroup{lim, start, count, grid});
+      LimGroup g{lim, start, count, {0, 0}};
+      for (int h = 0; h < 2; h++)
+        g.grid[h] = (int)std::min<long long>((count + c->cta_warps - 1) / c->cta_warps,
+                                             (long long)c->nsm * c->ctas_per_sm[h]);
+      c->groups.push_back(g);
     }
   }
 }
@@ -408,8 +415,8 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
     a.heun = heun;
     a.rlx = c->rlx;
     a.rlx_read = heun == 1 && rlx_read;
-    cudaError_t e = c->fast ? fastmath::launch_stage(g.lim, a, g.grid, st)
-                            : bitwise::launch_stage(g.lim, a, g.grid, st);
+    cudaError_t e = c->fast ? fastmath::launch_stage(g.lim, a, g.grid[heun], st)
+                            : bitwise::launch_stage(g.lim, a, g.grid[heun], st);
     if (e != cudaSuccess) return e;
   }
   for (int k = 1; k < ng; k++) {
@@ -471,7 +478,8 @@ static int autotune(mbm_ctx* c) {
   }
   int limmix = 0;
   for (const LimGroup& g : c->groups) limmix |= 1 << g.lim;
-  const auto key = std::make_tuple(strip_rows, c->nblk, limmix, c->ctas_per_sm);
+  const auto key = std::make_tuple(strip_rows, c->nblk, limmix,
+                                   (c->ctas_per_sm[0] * 256 + c->ctas_per_sm[1]) * c->cta_warps);
   {
     std::lock_guard<std::mutex> g(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -501,16 +509,19 @@ static int autotune(mbm_ctx* c) {
   // items, 4 waves) 1.7 % faster than 22.
   std::vector<double> cand;
   for (int seg = 8; seg <= 64; seg += 2) cand.push_back(seg);
-  const long long W = (long long)c->nsm * c->ctas_per_sm * CTA_WARPS;
-  const long long most = count_items(c, 8.0), least = count_items(c, 64.0);
-  for (long long k = (least + W - 1) / W; k * W < most && k <= 64; k++) {
-    double lo = 8.0, hi = 64.0;              // count_items(hi) <= k W < count_items(lo)
-    for (int it = 0; it < 40; it++) {
-      const double mid = 0.5 * (lo + hi);
-      if (count_items(c, mid) <= k * W) hi = mid;
-      else lo = mid;
+  for (int h = 0; h < 2; h++) {              // the resident warps of each stage
+    if (h == 1 && c->ctas_per_sm[1] == c->ctas_per_sm[0]) break;
+    const long long W = (long long)c->nsm * c->ctas_per_sm[h] * c->cta_warps;
+    const long long most = count_items(c, 8.0), least = count_items(c, 64.0);
+    for (long long k = (least + W - 1) / W; k * W < most && k <= 64; k++) {
+      double lo = 8.0, hi = 64.0;              // count_items(hi) <= k W < count_items(lo)
+      for (int it = 0; it < 40; it++) {
+        const double mid = 0.5 * (lo + hi);
+        if (count_items(c, mid) <= k * W) hi = mid;
+        else lo = mid;
+      }
+      cand.push_back(hi);
     }
-    cand.push_back(hi);
   }
   for (double seg : cand) {
     st = set_segments(c, seg);
@@ -718,7 +729,9 @@ static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vecto
 
   // work table and grid
   CKC(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device));
-  c->ctas_per_sm = c->fast ? fastmath::stage_ctas_per_sm() : bitwise::stage_ctas_per_sm();
+  for (int hh = 0; hh < 2; hh++)
+    c->ctas_per_sm[hh] = c->fast ? fastmath::stage_ctas_per_sm(hh) : bitwise::stage_ctas_per_sm(hh);
+  c->cta_warps = c->fast ? fastmath::stage_cta_warps() : bitwise::stage_cta_warps();
   long long max_items = 0;
   for (auto& d : c->hblk) max_items += (long long)((d.nxp - 3 + STRIP - 1) / STRIP) * ((d.nyp - 3 + 7) / 8 + 1);
   CKC(cudaMalloc(&c->dwork, sizeof(Work) * std::max<long long>(1, max_items)));
@@ -1106,7 +1119,7 @@ extern "C" int mbm_steps(mbm_ctx* c, double* t, double tend, double CFLmax, doub
 extern "C" int mbm_config(mbm_ctx* c, int* segment_rows, int* work_items, int* ctas) {
   if (!c) return fail(c, MBM_EINVAL, "mbm_config: null context");
   int g = 0;
-  for (const LimGroup& x : c->groups) g = std::max(g, x.grid);
+  for (const LimGroup& x : c->groups) g = std::max(g, std::max(x.grid[0], x.grid[1]));
   if (segment_rows) *segment_rows = (int)std::lround(c->seg_rows);
   if (work_items) *work_items = c->nwork;
   if (ctas) *ctas = g;
@@ -1729,9 +1742,10 @@ extern "C" int mbm_shard_control(mbm_ctx* c, int* done) {
   if (st) return st;
   CK(cudaSetDevice(c->device));
   CK(launch_control_ext(c->dcase, c->dblk, c->dlam, c->dtrace, c->dqueue, c->shard_cfl, c->stream));
+  if (!done) return MBM_OK;    // enqueued only: attempts after the last one are no-ops on the device
   CK(cudaMemcpyAsync(c->hcase, c->dcase, sizeof(CaseDev), cudaMemcpyDeviceToHost, c->stream));
   if ((st = wait_stream(c))) return st;
-  if (done) *done = c->hcase[0].done;
+  *done = c->hcase[0].done;
   return MBM_OK;
 }
 

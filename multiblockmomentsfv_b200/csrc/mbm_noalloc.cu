@@ -36,7 +36,8 @@
 namespace mbm {
 namespace bitwise {
 cudaError_t launch_stage(int lim, const StageArgs& a, int grid, cudaStream_t s);
-int stage_ctas_per_sm();
+int stage_ctas_per_sm(int heun);
+int stage_cta_warps();
 }
 void set_global_error(const std::string& msg);   // read back by mbm_last_error(NULL)
 }  // namespace mbm
@@ -185,7 +186,8 @@ extern "C" int mbm_stage_noalloc(const mbm_block_desc* blocks, int nblocks, cons
   a.sel_in = SEL_CUR;
   a.sel_d0 = heun ? SEL_TMP : SEL_CUR;
   a.sel_out = SEL_OTHER;
-  const long long grid = std::min<long long>((nwork + 3) / 4, (long long)sm * bitwise::stage_ctas_per_sm());
+  const int cw = bitwise::stage_cta_warps();
+  const long long grid = std::min<long long>((nwork + cw - 1) / cw, (long long)sm * bitwise::stage_ctas_per_sm(heun));
   e = bitwise::launch_stage(limiter, a, (int)grid, s);
   if (!e) e = cudaMemcpyAsync(h_lam, dlam, sizeof(unsigned long long) * 6 * nblocks, cudaMemcpyDeviceToHost, s);
   if (!e) e = cudaMemcpyAsync(&h_nonfinite, (const unsigned char*)dcase + offsetof(CaseDev, nonfinite), sizeof(int),

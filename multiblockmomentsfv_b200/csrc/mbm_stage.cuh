@@ -21,6 +21,7 @@
 #include <stdint.h>
 
 #include <mutex>
+#include <type_traits>
 
 #include "mbm_internal.h"
 #include "mbm_math.cuh"
@@ -43,14 +44,19 @@ __device__ __forceinline__ void load_cell(const double* __restrict__ base, long 
 
 // Rolling state of one warp, lane fastest (conflict-free 8-byte accesses): the
 // projected primitives of three consecutive rows, the lower state of the next
-// y face and the y flux of the face below the row being finished.
-struct WarpWindow {
+// y face and the y flux of the face below the row being finished.  Stage 2 adds two
+// slots its asynchronous copies land in (stage 1 prefetches into registers).
+struct WarpWindow1 {
   double P[3][NV][32];
   double lo[NV][32];
   double G[NV][32];
-  double Ua[NV][32];      // stage 2: the moments of the next row (asynchronous copies)
-  double D0a[NV][32];     // stage 2: Data0 of the next update row (asynchronous copies)
 };
+struct WarpWindow2 : WarpWindow1 {
+  double Ua[NV][32];      // the moments of the next row
+  double D0a[NV][32];     // Data0 (or its stored relaxation term) of the next update row
+};
+template <int HEUN>
+using WarpWindow = typename std::conditional<HEUN == 1, WarpWindow2, WarpWindow1>::type;
 
 // per-thread asynchronous 8-byte copy global -> shared (cp.async), and its groups
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
@@ -60,14 +66,17 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-constexpr int STAGE_WARPS = CTA_WARPS;
+#ifndef STAGE_CTA_WARPS
+#define STAGE_CTA_WARPS CTA_WARPS   // warps per CTA of this instantiation
+#endif
+constexpr int STAGE_WARPS = STAGE_CTA_WARPS;
 #ifndef STAGE_MIN_CTAS
 #define STAGE_MIN_CTAS 3   // CTAs per SM the register budget is sized for (168 registers)
 #endif
 
 template <int HEUN, int LIM>
 __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, const int lane,
-                                           WarpWindow& win) {
+                                           WarpWindow<HEUN>& win) {
   const BlockDev B = a.blk[w.blk];
   const CaseDev& cs = a.cases[B.case_id];
   if (cs.done) return;
@@ -116,7 +125,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   // one group per fetch, committed even when empty, so that the groups alternate
   // U(r), D0(r-2), U(r+1), D0(r-1), ... and each wait leaves only the newest in flight
   auto u_fetch = [&](int rr) {
-    if (HEUN == 1) {
+    if constexpr (HEUN == 1) {
       if (col_in && rr >= 0 && rr < nyp) {
         const long long idx = (long long)rr * pitch + C + 1;
 #pragma unroll
@@ -126,7 +135,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     }
   };
   auto d0_fetch = [&](int Jn) {
-    if (HEUN == 1) {
+    if constexpr (HEUN == 1) {
       if (col_out && Jn >= NG && Jn <= nyp - 1 - NG && Jn >= w.J0 && Jn < w.J1) {
         const long long idx = (long long)Jn * pitch + C + 1;
 #pragma unroll
@@ -155,7 +164,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         const bool okn = col_in && r + 1 >= 0 && r + 1 < nyp;
         if (okn) load_cell(in, plane, (long long)(r + 1) * pitch + C + 1, Un);
         else benign(Un);
-      } else {
+      } else if constexpr (HEUN == 1) {
         cp_async_wait_one();                 // this row's moments have landed
         if (ok) {
 #pragma unroll
@@ -348,7 +357,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         primitive(U, Q);
         relax<2 * HEUN>(Q, R, dt, Kn, Fx);
 #endif
-        if (HEUN == 1) {
+        if constexpr (HEUN == 1) {
           double R0[NV];
 #pragma unroll
           for (int n = 0; n < NV; n++) U[n] = win.D0a[n][lane];
@@ -410,14 +419,23 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
 // Persistent grid (as many CTAs as fit on the SMs); every warp takes the next work
 // item from a counter until the table is exhausted, so uneven blocks and the last
 // wave balance themselves.
-// the windows live in dynamic shared memory (STAGE_SMEM bytes, above the 48 KB a static
-// allocation may take)
-constexpr int STAGE_SMEM = (int)sizeof(WarpWindow) * STAGE_WARPS;
+// the windows live in dynamic shared memory (stage_smem<HEUN> bytes, above the 48 KB a
+// static allocation may take)
+template <int HEUN>
+constexpr int stage_smem() { return (int)sizeof(WarpWindow<HEUN>) * STAGE_WARPS; }
 
+// register budget: STAGE_MAXNREG caps the registers per thread directly (for CTAs of
+// one warp, whose residency the minimum-CTA form of the bound describes poorly);
+// otherwise the launch bound asks for STAGE_MIN_CTAS resident CTAs
+#ifdef STAGE_MAXNREG
+#define STAGE_BOUNDS __maxnreg__(STAGE_MAXNREG)
+#else
+#define STAGE_BOUNDS __launch_bounds__(32 * STAGE_WARPS, STAGE_MIN_CTAS)
+#endif
 template <int HEUN, int LIM>
-__global__ void __launch_bounds__(32 * STAGE_WARPS, STAGE_MIN_CTAS) stage_kernel(const StageArgs a) {
-  extern __shared__ __align__(16) unsigned char stage_smem[];
-  WarpWindow* win = reinterpret_cast<WarpWindow*>(stage_smem);
+__global__ void STAGE_BOUNDS stage_kernel(const StageArgs a) {
+  extern __shared__ __align__(16) unsigned char stage_shared[];
+  WarpWindow<HEUN>* win = reinterpret_cast<WarpWindow<HEUN>*>(stage_shared);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (;;) {
     int w = 0;
@@ -430,13 +448,13 @@ __global__ void __launch_bounds__(32 * STAGE_WARPS, STAGE_MIN_CTAS) stage_kernel
 
 template <int HEUN, int LIM>
 static void smem_attr() {
-  cudaFuncSetAttribute(stage_kernel<HEUN, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM);
+  cudaFuncSetAttribute(stage_kernel<HEUN, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_smem<HEUN>());
 }
 
 // called at context creation (the device current), before any launch or graph capture:
 // allows the dynamic shared memory for every instantiation on this device, then asks
-// how many CTAs fit per SM
-int stage_ctas_per_sm() {
+// how many CTAs of Heun stage `heun` fit per SM
+int stage_ctas_per_sm(int heun) {
   static std::mutex mu;
   static unsigned long long done = 0;     // one bit per device ordinal < 64
   int dev = 0;
@@ -451,18 +469,23 @@ int stage_ctas_per_sm() {
     }
   }
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<1, 4>, 32 * STAGE_WARPS, STAGE_SMEM);
+  if (heun)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<1, 4>, 32 * STAGE_WARPS, stage_smem<1>());
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<0, 4>, 32 * STAGE_WARPS, stage_smem<0>());
   return n > 0 ? n : 1;
 }
+
+int stage_cta_warps() { return STAGE_WARPS; }
 
 template <int HEUN>
 static cudaError_t launch_stage_lim(int lim, const StageArgs& a, int grid, cudaStream_t s) {
   switch (lim) {
-    case 0: stage_kernel<HEUN, 0><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
-    case 1: stage_kernel<HEUN, 1><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
-    case 2: stage_kernel<HEUN, 2><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
-    case 3: stage_kernel<HEUN, 3><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
-    default: stage_kernel<HEUN, 4><<<grid, 32 * STAGE_WARPS, STAGE_SMEM, s>>>(a); break;
+    case 0: stage_kernel<HEUN, 0><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
+    case 1: stage_kernel<HEUN, 1><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
+    case 2: stage_kernel<HEUN, 2><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
+    case 3: stage_kernel<HEUN, 3><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
+    default: stage_kernel<HEUN, 4><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
   }
   return cudaGetLastError();
 }

@@ -162,7 +162,11 @@ class ShardPart:
     def cfl(self):
         self._check(self.L.mbm_shard_cfl(self.ctx))
 
-    def control(self) -> int:
+    def control(self, wait: bool = True) -> Optional[int]:
+        """The controller of the attempt; wait=False enqueues it and returns None."""
+        if not wait:
+            self._check(self.L.mbm_shard_control(self.ctx, None))
+            return None
         d = C.c_int(0)
         self._check(self.L.mbm_shard_control(self.ctx, C.byref(d)))
         return d.value
@@ -251,25 +255,30 @@ def initialise(parts: Sequence[ShardPart], scenario: sc.Scenario, ex) -> None:
 
 
 def steps(parts: Sequence[ShardPart], ex, t: float, tend: float, CFLmax: float = 1.0,
-          CFLreg: Optional[float] = None, max_steps: int = 0):
-    """Steps() over the split case; returns (t, accepted steps, rejected attempts)."""
+          CFLreg: Optional[float] = None, max_steps: int = 0, batch: int = 8):
+    """Steps() over the split case; returns (t, accepted steps, rejected attempts).
+    Attempts are enqueued `batch` at a time, and the host reads the end flag once per
+    batch (attempts after the last one return at once on the device); every rank
+    enqueues the same attempts, exchanges and reductions."""
     CFLreg = parts[0].deck.CFL if CFLreg is None else CFLreg
     for p in parts:
         p.begin(t, tend, CFLmax, CFLreg, max_steps)
     done = not (t < tend)
+    nb = max(1, batch)
     while not done:
-        for heun, out in ((0, L_TMP), (1, L_NEW)):
+        for k in range(nb):
+            for heun, out in ((0, L_TMP), (1, L_NEW)):
+                for p in parts:
+                    p.stage(heun)
+                for p in parts:
+                    p.pack(out)
+                ex.move(parts)
+                for p in parts:
+                    p.fill(out)
             for p in parts:
-                p.stage(heun)
-            for p in parts:
-                p.pack(out)
-            ex.move(parts)
-            for p in parts:
-                p.fill(out)
-        for p in parts:
-            p.cfl()
-        ex.reduce_max(parts)
-        flags = [p.control() for p in parts]
+                p.cfl()
+            ex.reduce_max(parts)
+            flags = [p.control(wait=k == nb - 1) for p in parts]
         if len(set(flags)) != 1:
             raise RuntimeError("ranks disagree on the end of the step loop")
         done = bool(flags[0])
