@@ -81,18 +81,23 @@ __device__ __forceinline__ bool inner(const BlockDev& B, int I, int J) {
   return I >= NG && I <= B.nxp - 1 - NG && J >= NG && J <= B.nyp - 1 - NG;
 }
 
-// limited slope of cell (I,J) along dir from the primitives (src/Main.c:346-349)
+// limited slope of cell (I,J) along dir from the primitives (src/Main.c:346-349).  The
+// face and cell passes are specialised per Heun stage and limiter (HEUN, LIM), as the
+// forward stage kernel is: the limiter's branches and the stage's relaxation flags fold
+// away at compile time.
+template <int LIM>
 __device__ __forceinline__ double slope_at(const AdjArgs& a, const BlockDev& B, int I, int J, int dir, int m,
                                           double h) {
   const long long i = cidx(B, I, J) + m * B.plane;
   const long long s = dir == 1 ? 1 : B.pitch;
   const double d1 = a.P[i] - a.P[i - s], d2 = a.P[i + s] - a.P[i];
-  return mbm_adj::limit_val(a.limiter, d1, d2) * mbm_adj::rcp(h);
+  return mbm_adj::limit_val(LIM, d1, d2) * mbm_adj::rcp(h);
 }
 
 // pass B: faces (I,J)|(I+1,J) (dir 1) or (I,J)|(I,J+1) (dir 2) next to an output cell
 // 128 registers: four 128-thread CTAs per SM hide the neighbour loads better than
 // the spill-free allocation at half the occupancy
+template <int HEUN, int LIM>
 __device__ __forceinline__ void face_adj(const AdjArgs& a, const BlockDev& B, int I, int J, int dir,
                                          double* __restrict__ FL, double* __restrict__ FR) {
   const int I2 = dir == 1 ? I + 1 : I, J2 = dir == 1 ? J : J + 1;
@@ -108,7 +113,7 @@ __device__ __forceinline__ void face_adj(const AdjArgs& a, const BlockDev& B, in
     return;
   }
   const double h = dir == 1 ? B.dx : B.dy, rh = mbm_adj::rcp(h);
-  const double s = a.heun ? 0.5 : 1.0;
+  const double s = HEUN ? 0.5 : 1.0;
   double PL[NV], PR[NV], fb[NV], gl[NV] = {0}, gr[NV] = {0};
   bool any = false;
   for (int m = 0; m < NV; m++) {
@@ -116,8 +121,8 @@ __device__ __forceinline__ void face_adj(const AdjArgs& a, const BlockDev& B, in
     const double hi = inR ? a.lout[cidx(B, I2, J2) + m * B.plane] : 0.0;
     fb[m] = s * a.dt * rh * (hi - lo);
     any = any || fb[m] != 0.0;
-    PL[m] = a.P[cidx(B, I, J) + m * B.plane] + 0.5 * h * slope_at(a, B, I, J, dir, m, h);
-    PR[m] = a.P[cidx(B, I2, J2) + m * B.plane] - 0.5 * h * slope_at(a, B, I2, J2, dir, m, h);
+    PL[m] = a.P[cidx(B, I, J) + m * B.plane] + 0.5 * h * slope_at<LIM>(a, B, I, J, dir, m, h);
+    PR[m] = a.P[cidx(B, I2, J2) + m * B.plane] - 0.5 * h * slope_at<LIM>(a, B, I2, J2, dir, m, h);
   }
   if (any) mbm_adj::hll_p_adj(PL, PR, fb, gl, gr, dir);
   const long long i = cidx(B, I, J);
@@ -129,14 +134,15 @@ __device__ __forceinline__ void face_adj(const AdjArgs& a, const BlockDev& B, in
 }
 
 // both faces of a cell that lie on its high side: (I,J)|(I+1,J) and (I,J)|(I,J+1)
+template <int HEUN, int LIM>
 __global__ void __launch_bounds__(128, 4) adj_faces(AdjArgs a, long long nthr, double* FLx, double* FRx,
                                                     double* FLy, double* FRy) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, J;
   if (k >= nthr || !locate(a.blk, a.nblk, k, b, I, J)) return;
   const BlockDev B = a.blk[b];
-  face_adj(a, B, I, J, 1, FLx, FRx);
-  face_adj(a, B, I, J, 2, FLy, FRy);
+  face_adj<HEUN, LIM>(a, B, I, J, 1, FLx, FRx);
+  face_adj<HEUN, LIM>(a, B, I, J, 2, FLy, FRy);
 }
 
 // adjoint of the reconstruction and slopes along one direction, accumulated into Pb;
@@ -144,6 +150,7 @@ __global__ void __launch_bounds__(128, 4) adj_faces(AdjArgs a, long long nthr, d
 // component are issued before any arithmetic; the slope terms of a neighbour are
 // skipped when its slope adjoint is zero (cells no output depends on may hold no
 // state, and 0 * NaN would leak into the sum)
+template <int LIM>
 __device__ __forceinline__ void gather_dir(const AdjArgs& a, const BlockDev& B, int I, int J, int dir,
                                            const double* FL, const double* FR, double* Pb) {
   const long long s = dir == 1 ? 1 : B.pitch;
@@ -165,19 +172,19 @@ __device__ __forceinline__ void gather_dir(const AdjArgs& a, const BlockDev& B, 
     const double l0 = 0.5 * h * (fl0 - frm);
     if (l0 != 0.0) {
       double g1, g2;
-      mbm_adj::limit_grad(a.limiter, p0 - pm, pp - p0, &g1, &g2);
+      mbm_adj::limit_grad(LIM, p0 - pm, pp - p0, &g1, &g2);
       g += l0 * (g1 - g2) * rh;
     }
     const double lm = lft ? 0.5 * h * (flm - frm2) : 0.0;
     if (lm != 0.0) {
       double g1, g2;
-      mbm_adj::limit_grad(a.limiter, pm - pm2, p0 - pm, &g1, &g2);
+      mbm_adj::limit_grad(LIM, pm - pm2, p0 - pm, &g1, &g2);
       g += lm * g2 * rh;
     }
     const double lp = rgt ? 0.5 * h * (flp - fr0) : 0.0;
     if (lp != 0.0) {
       double g1, g2;
-      mbm_adj::limit_grad(a.limiter, pp - p0, pp2 - pp, &g1, &g2);
+      mbm_adj::limit_grad(LIM, pp - p0, pp2 - pp, &g1, &g2);
       g -= lp * g1 * rh;
     }
     Pb[m] += g;
@@ -186,14 +193,15 @@ __device__ __forceinline__ void gather_dir(const AdjArgs& a, const BlockDev& B, 
 
 // pass C: per cell, back to the stage input (and Data0)
 // one cell's share; returns its contribution to dJ/dKn
+template <int HEUN, int LIM>
 __device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, int I, int J, const double* FLx,
                                            const double* FRx, const double* FLy, const double* FRy) {
   double Pb[NV] = {0}, Ub[NV] = {0}, U[NV], P0[NV];
   double knb = 0.0;
   const bool ring = I == 0 || J == 0 || I == B.nxp - 1 || J == B.nyp - 1;
   if (!ring) {
-    gather_dir(a, B, I, J, 1, FLx, FRx, Pb);
-    gather_dir(a, B, I, J, 2, FLy, FRy, Pb);
+    gather_dir<LIM>(a, B, I, J, 1, FLx, FRx, Pb);
+    gather_dir<LIM>(a, B, I, J, 2, FLy, FRy, Pb);
   }
   load9(a.x, B, I, J, U);
   mbm_adj::prim(U, P0);
@@ -202,20 +210,20 @@ __device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, 
 #pragma unroll
   for (int m = 0; m < NV; m++) anyP = anyP || Pb[m] != 0.0;
   if (anyP) {     // Aux = relax(Primitive(U), 2H+1) off the ring (ring cells never reach a face)
-    mbm_adj::relax_p_adj(P0, Pb, Qb, &knb, a.dt, a.Kn, 2 * a.heun + 1);
+    mbm_adj::relax_p_adj(P0, Pb, Qb, &knb, a.dt, a.Kn, 2 * HEUN + 1);
   }
   const long long ic = cidx(B, I, J);
   double Vb[NV] = {0};
   if (inner(B, I, J)) {
     // update term R: Conservative(relax(Primitive(X), 2H)) [+ Conservative(relax(Primitive(D0), -1))]
-    const double s = a.heun ? 0.5 : 1.0;
+    const double s = HEUN ? 0.5 : 1.0;
     double Rb[NV], Q[NV], Cb[NV] = {0};
 #pragma unroll
     for (int m = 0; m < NV; m++) Rb[m] = s * a.lout[cidx(B, I, J) + m * B.plane];
-    mbm_adj::relax_p(P0, Q, a.dt, a.Kn, a.F, 2 * a.heun);
+    mbm_adj::relax_p(P0, Q, a.dt, a.Kn, a.F, 2 * HEUN);
     mbm_adj::cons_adj(Q, Rb, Cb);
-    mbm_adj::relax_p_adj(P0, Cb, Qb, &knb, a.dt, a.Kn, 2 * a.heun);
-    if (a.heun) {
+    mbm_adj::relax_p_adj(P0, Cb, Qb, &knb, a.dt, a.Kn, 2 * HEUN);
+    if (HEUN) {
       double V[NV], W[NV], Q2[NV], C2[NV] = {0}, Pd[NV] = {0};
       load9(a.d0, B, I, J, V);
       mbm_adj::prim(V, W);
@@ -231,7 +239,7 @@ __device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, 
   if (anyQ) mbm_adj::prim_adj(U, Qb, Ub);   // cells no stage output depends on may hold no state
   // stage 2 starts both adjoint layers (every cell written: no clearing pass), stage 1
   // adds to the layer stage 2 started
-  if (a.heun) {
+  if (HEUN) {
 #pragma unroll
     for (int m = 0; m < NV; m++) {
       a.lx[ic + m * B.plane] = Ub[m];
@@ -246,13 +254,15 @@ __device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, 
 
 // 64 registers, eight 128-thread CTAs per SM: the pass waits on its neighbour loads, and
 // more loads in flight pay for the spills (measured, 4 x 256^2: 8 CTAs 10 % faster than 4)
+template <int HEUN, int LIM>
 __global__ void __launch_bounds__(128, 8) adj_cells(AdjArgs a, long long nthr, const double* FLx,
                                                     const double* FRx, const double* FLy, const double* FRy) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, J;
   double knb = 0.0;
   // threads past a block's edge stay for the warp sum below
-  if (k < nthr && locate(a.blk, a.nblk, k, b, I, J)) knb = cell_adj(a, a.blk[b], I, J, FLx, FRx, FLy, FRy);
+  if (k < nthr && locate(a.blk, a.nblk, k, b, I, J))
+    knb = cell_adj<HEUN, LIM>(a, a.blk[b], I, J, FLx, FRx, FLy, FRy);
   // the Kn derivative: warp sum, one atomic per warp
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) knb += __shfl_xor_sync(0xffffffffu, knb, o);
@@ -587,13 +597,32 @@ cudaError_t adjoint_stage_march(const AdjArgs& a, int grid, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <int HEUN, int LIM>
+static void faces_cells(const AdjArgs& a0, long long nthr, unsigned G, double* FLx, double* FRx, double* FLy,
+                        double* FRy, cudaStream_t s) {
+  adj_faces<HEUN, LIM><<<G, 128, 0, s>>>(a0, nthr, FLx, FRx, FLy, FRy);
+  adj_cells<HEUN, LIM><<<G, 128, 0, s>>>(a0, nthr, FLx, FRx, FLy, FRy);
+}
+
+template <int HEUN>
+static void faces_cells_lim(const AdjArgs& a0, long long nthr, unsigned G, double* FLx, double* FRx,
+                            double* FLy, double* FRy, cudaStream_t s) {
+  switch (a0.limiter) {
+    case 0: faces_cells<HEUN, 0>(a0, nthr, G, FLx, FRx, FLy, FRy, s); break;
+    case 1: faces_cells<HEUN, 1>(a0, nthr, G, FLx, FRx, FLy, FRy, s); break;
+    case 2: faces_cells<HEUN, 2>(a0, nthr, G, FLx, FRx, FLy, FRy, s); break;
+    case 3: faces_cells<HEUN, 3>(a0, nthr, G, FLx, FRx, FLy, FRy, s); break;
+    default: faces_cells<HEUN, 4>(a0, nthr, G, FLx, FRx, FLy, FRy, s); break;
+  }
+}
+
 cudaError_t adjoint_stage(const AdjArgs& a0, long long nthr, double* FLx, double* FRx, double* FLy,
                           double* FRy, cudaStream_t s) {
   const int T = 128;
   const unsigned G = (unsigned)(nthr / T);
   adj_prims<<<G, T, 0, s>>>(a0, nthr);
-  adj_faces<<<G, T, 0, s>>>(a0, nthr, FLx, FRx, FLy, FRy);
-  adj_cells<<<G, T, 0, s>>>(a0, nthr, FLx, FRx, FLy, FRy);
+  if (a0.heun) faces_cells_lim<1>(a0, nthr, G, FLx, FRx, FLy, FRy, s);
+  else faces_cells_lim<0>(a0, nthr, G, FLx, FRx, FLy, FRy, s);
   return cudaGetLastError();
 }
 
