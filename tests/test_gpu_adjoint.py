@@ -92,6 +92,64 @@ def test_adjoint_benchmark_case():
     assert errK < 1e-6, errK
 
 
+def test_adjoint_benchmark_case_harmonic():
+    """The case the bench's adjoint leg times: 4 blocks x 256^2, 200 steps, checkpoints
+    every 20, harmonic limiter, fast forward; 16 seeded directions at eps = 1e-6 and
+    1e-8.  The harmonic limiter's weights |d| + 1e-10 have a kink where a one-sided
+    difference d changes sign, and there the slope's derivative jumps by O(1); a
+    central difference of step eps crosses such kinks (about 7e-4 of the one-sided
+    differences per step change sign between the +eps and -eps runs of this case), so
+    its error is that of the crossings, and it falls with eps -- a wrong adjoint
+    would leave an error that does not.  Measured: median relative error 1.2e-3 at
+    eps = 1e-6 (worst 1.4e-2), 6.1e-5 at 1e-8 (worst 4.6e-4)."""
+    n, nsteps, every, seed = 256, 200, 20, 11
+    d = H.quadrant_deck(n, Kn=0.01, limiter=bf.LIM_HARMONIC)
+    base = adj.smooth_base(d, seed)
+    rng = np.random.default_rng(seed)
+    th0 = _theta0(d, rng)
+    with adj.Sensitivity(d, base, mode="fast") as S:
+        layers = adj.state_from_theta(d, base, th0)
+        S.load(layers)
+        J, g, gK, dts, ms = S.run(nsteps, every)
+        gth = adj.theta_gradient(d, layers, g)
+        dirs = [[rng.standard_normal(t.shape) for t in th0] for _ in range(16)]
+        med, worst = {}, {}
+        for eps in (1e-6, 1e-8):
+            errs = []
+            for v in dirs:
+                S.load(adj.state_from_theta(d, base, [t + eps * w for t, w in zip(th0, v)]))
+                Jp = S.replay(dts)
+                S.load(adj.state_from_theta(d, base, [t - eps * w for t, w in zip(th0, v)]))
+                Jm = S.replay(dts)
+                fd = (Jp - Jm) / (2 * eps)
+                ad = sum(float(np.sum(a * w)) for a, w in zip(gth, v))
+                errs.append(abs(fd - ad) / abs(fd))
+            med[eps], worst[eps] = float(np.median(errs)), float(np.max(errs))
+        # kink crossings of the first direction: one-sided differences of the primitives
+        # whose sign differs between the +eps and -eps runs, over every step
+        eps, v = 1e-6, dirs[0]
+        signs = []
+        for sgn in (1.0, -1.0):
+            S.load(adj.state_from_theta(d, base, [t + sgn * eps * w for t, w in zip(th0, v)]))
+            run = []
+            for k in range(len(dts) + 1):
+                if k:
+                    S.replay(dts[k - 1:k])
+                for b in range(len(d.blocks)):
+                    P = output.primitive(S.s.download(sv.L_DATA, b)[bf.NG - 1:-bf.NG + 1, bf.NG - 1:-bf.NG + 1])
+                    run += [np.signbit(np.diff(P, axis=1)), np.signbit(np.diff(P, axis=0))]
+            signs.append(run)
+        flips = sum(int(np.count_nonzero(x != y)) for x, y in zip(*signs))
+        total = sum(x.size for x in signs[0])
+    print(f"harmonic adjoint check: eps 1e-6 median {med[1e-6]:.1e} worst {worst[1e-6]:.1e}; eps 1e-8 median "
+          f"{med[1e-8]:.1e} worst {worst[1e-8]:.1e}; kink crossings {flips / total:.1e} of one-sided differences; "
+          f"forward {ms[0]:.1f} ms, adjoint {ms[1]:.1f} ms")
+    assert flips > 0
+    assert med[1e-6] <= 5e-3 and worst[1e-6] <= 5e-2, (med, worst)
+    assert med[1e-8] <= 3e-4 and worst[1e-8] <= 2e-3, (med, worst)
+    assert med[1e-6] >= 5 * med[1e-8], med         # the error falls with eps
+
+
 def _oracle_replay(O, d, layers, dts):
     """J after the frozen-dt steps of the C oracle (TimeUpdate, then NEW -> DATA)."""
     o = O.Oracle(d, sc.Scenario.named("riemann2d"))
