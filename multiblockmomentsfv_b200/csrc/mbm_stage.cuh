@@ -44,19 +44,26 @@ __device__ __forceinline__ void load_cell(const double* __restrict__ base, long 
 
 // Rolling state of one warp, lane fastest (conflict-free 8-byte accesses): the
 // projected primitives of three consecutive rows, the lower state of the next
-// y face and the y flux of the face below the row being finished.  Stage 2 adds two
-// slots its asynchronous copies land in (stage 1 prefetches into registers).
+// y face and the y flux of the face below the row being finished.  Stage 2 adds three
+// slots its asynchronous copies land in (stage 1 prefetches into registers); stage 1
+// in fast arithmetic keeps the relaxation term of the last three rows, which the
+// update of the row two iterations later reads from here, not from global memory.
 struct WarpWindow1 {
   double P[3][NV][32];
   double lo[NV][32];
   double G[NV][32];
 };
+struct WarpWindowR : WarpWindow1 {
+  double R[3][NV][32];    // relax<-1> of rows r-2 .. r (the ring of P)
+};
 struct WarpWindow2 : WarpWindow1 {
   double Ua[NV][32];      // the moments of the next row
   double D0a[NV][32];     // Data0 (or its stored relaxation term) of the next update row
+  double UJa[NV][32];     // the moments of the next update row
 };
 template <int HEUN>
-using WarpWindow = typename std::conditional<HEUN == 1, WarpWindow2, WarpWindow1>::type;
+using WarpWindow = typename std::conditional<
+    HEUN == 1, WarpWindow2, typename std::conditional<MBM_FAST_ARITH != 0, WarpWindowR, WarpWindow1>::type>::type;
 
 // per-thread asynchronous 8-byte copy global -> shared (cp.async), and its groups
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
@@ -87,9 +94,9 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   const double* __restrict__ d0 = a.buf[phys_layer(a.sel_d0, cur)] + B.off;
   double* __restrict__ out = a.buf[phys_layer(a.sel_out, cur)] + B.off;
 #if MBM_FAST_ARITH
-  // the relaxation term of the stage-1 input: written by stage 1 at its row r and read
-  // back (plain loads: written in this launch) by the update of that row two
-  // iterations later; stage 2 reads it with rlx_read in place of forming it from Data0
+  // the relaxation term of the stage-1 input: written by stage 1 at its row r (also
+  // into the window, where the update of that row two iterations later reads it);
+  // stage 2 reads it with rlx_read in place of forming it from Data0
   double* __restrict__ rlx = a.rlx + B.off;
   const bool rlx_rd = HEUN == 1 && a.rlx_read;
   const double* __restrict__ d0src = rlx_rd ? rlx : d0;
@@ -121,7 +128,8 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   // which stage 2, holding Data0 as well, cannot spare without spilling).
   constexpr bool PREFETCH = HEUN == 0;
   // Stage 2 copies, without registers, the moments of row r+1 into shared memory while
-  // it works on row r, and Data0 of update row J+1 while it finishes row J (= r-2):
+  // it works on row r, and Data0 (or its relaxation term) and the moments of update row
+  // J+1 while it finishes row J (= r-2):
   // one group per fetch, committed even when empty, so that the groups alternate
   // U(r), D0(r-2), U(r+1), D0(r-1), ... and each wait leaves only the newest in flight
   auto u_fetch = [&](int rr) {
@@ -139,7 +147,10 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
       if (col_out && Jn >= NG && Jn <= nyp - 1 - NG && Jn >= w.J0 && Jn < w.J1) {
         const long long idx = (long long)Jn * pitch + C + 1;
 #pragma unroll
-        for (int n = 0; n < NV; n++) cp_async8(&win.D0a[n][lane], d0src + n * plane + idx);
+        for (int n = 0; n < NV; n++) {
+          cp_async8(&win.D0a[n][lane], d0src + n * plane + idx);
+          cp_async8(&win.UJa[n][lane], in + n * plane + idx);
+        }
       }
       cp_async_commit();
     }
@@ -190,7 +201,10 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
           relaxed_moments(Q, dm.d1_0, dm.d2_0, R0);
           const long long idx = (long long)r * pitch + C + 1;
 #pragma unroll
-          for (int n = 0; n < NV; n++) rlx[n * plane + idx] = R0[n];
+          for (int n = 0; n < NV; n++) {
+            rlx[n * plane + idx] = R0[n];
+            if constexpr (HEUN == 0) win.R[s0][n][lane] = R0[n];
+          }
         }
         if (!(col_ring || r == 0 || r == nyp - 1)) {
           const double th = Q[3];
@@ -338,11 +352,12 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         double U[NV], Q[NV], R[NV];
 #if MBM_FAST_ARITH
         const double g = dt * Fx;
-        if (HEUN == 1) {
-          load_cell(in, plane, idx, U);
+        if constexpr (HEUN == 1) {
+#pragma unroll
+          for (int n = 0; n < NV; n++) U[n] = win.UJa[n][lane];
         } else {
 #pragma unroll
-          for (int n = 0; n < NV; n++) U[n] = rlx[n * plane + idx];   // relax<-1> of this cell
+          for (int n = 0; n < NV; n++) U[n] = win.R[sm2][n][lane];    // relax<-1> of this cell
         }
         // stage 1: relax<0> = the force push of relax<-1>; stage 2: relax<2> = the force
         // push of the moments (both the identity without a force)
@@ -353,7 +368,12 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
           for (int n = 0; n < NV; n++) R[n] = U[n];
         }
 #else
-        load_cell(in, plane, idx, U);
+        if constexpr (HEUN == 1) {
+#pragma unroll
+          for (int n = 0; n < NV; n++) U[n] = win.UJa[n][lane];
+        } else {
+          load_cell(in, plane, idx, U);
+        }
         primitive(U, Q);
         relax<2 * HEUN>(Q, R, dt, Kn, Fx);
 #endif
