@@ -5,14 +5,21 @@ block 3 bottom), extrapolation on every outer edge, R13 = 1, Kn = 0.005, superbe
 the 2D temperature-Riemann initial state, to t = 0.6.
 
 At this size the oracle runs a few steps in seconds: three Steps of the bitwise GPU
-path equal it bit for bit (states, step count, end time).  To t = 0.6 (2,348 steps)
-the fast mode is held to the bitwise mode (itself equal to the reference) within
-1e-8 per field (max |a - b| over max |b|; measured 1.5e-9).  The reference's
-pointwise regression gate (|a - b| <= 1e-10 + 1e-8 |b|, tools/compare_solution.py)
-is applied to its own deck (test_gpu_fast, test_gpu_dropin); after 2,348 superbee
-steps it is exceeded at 568 of 8.9 M values (0.006 %), values far below their field's
-maximum, where the 1e-10 floor is smaller than an error of 1e-9 of the field's scale;
-this test reports the count."""
+path equal it bit for bit (states, step count, end time).  The bitwise mode is the
+reference's arithmetic, so to t = 0.6 it meets any gate against the reference with no
+difference at all.
+
+The reference's own result on this deck is sensitive at the level its regression gate
+(|a - b| <= 1e-10 + 1e-8 |b|, tools/compare_solution.py) tests: the same run from an
+initial state perturbed by relative 1e-15 noise (the bitwise mode is the reference)
+exceeds the gate from t = 0.3 on at hundreds to thousands of values (at t = 0.6: 231,
+765 and 723 for three seeds; per-field error up to 1.6e-9 of the field's maximum, and
+above 1e-8 at t = 0.5).  Up to t = 0.2 the fast mode passes the gate (the reference's
+tool says PASS); at t = 0.6 no arithmetic but the reference's own can pass it, and the
+fast mode is held to the reference's own spread instead: its per-field error within
+1e-8, and its count of values beyond the gate within twice the largest of three 1e-15
+perturbations of the reference (measured 428 against 765).  The reference's tool, run
+on the written files, agrees with those counts."""
 import numpy as np
 import pytest
 
@@ -67,7 +74,41 @@ def test_lshape512_steps_bitwise(oracle_mod):
         H.assert_bitwise(got[b], ref[b], f"block {b + 1}")
 
 
-def test_lshape512_fast_to_end_time():
+def _perturbed(d, scn, tend, seed, eps=1e-15):
+    """The bitwise run from an initial state perturbed by relative noise of size eps."""
+    with sv.Solver(d, scn, mode="exact", show_every=0) as s:
+        s.initialise()
+        rng = np.random.default_rng(seed)
+        for b in range(len(d.blocks)):
+            U = s.download(sv.L_DATA, b)
+            s.upload(sv.L_DATA, b, U * (1.0 + eps * rng.uniform(-1.0, 1.0, U.shape)))
+        t, n, r = s.steps(0.0, tend)
+        return s.layers(sv.L_DATA), t, n, r
+
+
+def _gate_count(a, b):
+    return sum(int(np.count_nonzero(np.abs(x - y) > 1e-10 + 1e-8 * np.abs(y))) for x, y in zip(a, b))
+
+
+def _write(tmp_path, name, d, layers, t):
+    w = output.Writer(str(tmp_path / name), d, "Riemann2D", single=False)
+    w.write(layers, t, -1)
+    return w.base
+
+
+def test_lshape512_fast_passes_the_gate_to_t02(tmp_path):
+    """Up to t = 0.2 (about 780 steps) the fast mode passes the reference's regression
+    gate at its Float64 defaults, run as the reference's own tool (measured: no value
+    beyond it, largest per-field error 9e-12 of the field's maximum)."""
+    d, scn = lshape512(), sc.Scenario.named("riemann2d")
+    ref, t0, n0, r0 = _run(d, scn, "exact", 0.2)
+    fast, t1, n1, r1 = _run(d, scn, "fast", 0.2)
+    assert (t0, n0, r0) == (t1, n1, r1)
+    ok, log = H.reference_compare(_write(tmp_path, "fast", d, fast, t1), _write(tmp_path, "exact", d, ref, t0))
+    assert ok and log.startswith("PASS"), log
+
+
+def test_lshape512_fast_to_end_time(tmp_path):
     d, scn = lshape512(), sc.Scenario.named("riemann2d")
     ref, t0, n0, r0 = _run(d, scn, "exact", TEND)
     fast, t1, n1, r1 = _run(d, scn, "fast", TEND)
@@ -76,8 +117,20 @@ def test_lshape512_fast_to_end_time():
     num = np.max([np.abs(x - y).reshape(-1, 10).max(axis=0) for x, y in zip(a, b)], axis=0)
     den = np.max([np.abs(y).reshape(-1, 10).max(axis=0) for y in b], axis=0)
     err = num / den
-    bad = sum(int(np.count_nonzero(np.abs(x - y) > 1e-10 + 1e-8 * np.abs(y))) for x, y in zip(a, b))
+    bad_fast = _gate_count(a, b)
+    # the reference's own spread: the bitwise run from three perturbed initial states
+    spread = []
+    for seed in (1, 2, 3):
+        pert, t2, n2, r2 = _perturbed(d, scn, TEND, seed)
+        spread.append(_gate_count(_fields(pert), b))
     total = sum(x.size for x in a)
-    print("L-shape 512/unit to t = 0.6 (%d steps): fast vs exact max %.1e per field; pointwise gate "
-          "exceeded at %d of %d values" % (n0, err.max(), bad, total))
+    # the reference's own tool on the written result files (Float64) agrees with the counts
+    f_exact = _write(tmp_path, "exact", d, ref, TEND)
+    ok_fast, log_fast = H.reference_compare(_write(tmp_path, "fast", d, fast, TEND), f_exact)
+    ok_pert, log_pert = H.reference_compare(_write(tmp_path, "perturbed", d, pert, TEND), f_exact)
+    print("L-shape 512/unit to t = 0.6 (%d steps): fast vs exact max %.1e per field, %d of %d values beyond "
+          "the gate; the reference from 1e-15-perturbed states: %s; reference tool: fast %s, perturbed %s"
+          % (n0, err.max(), bad_fast, total, spread, log_fast.split(":")[0], log_pert.split(":")[0]))
     assert err.max() <= 1e-8, err
+    assert ok_fast == (bad_fast == 0) and ok_pert == (spread[-1] == 0)
+    assert bad_fast <= 2 * max(max(spread), 1), (bad_fast, spread)
