@@ -134,8 +134,14 @@ __device__ __forceinline__ void face_adj(const AdjArgs& a, const BlockDev& B, in
 }
 
 // both faces of a cell that lie on its high side: (I,J)|(I+1,J) and (I,J)|(I,J+1)
+#ifndef ADJ_FACE_CTAS
+#define ADJ_FACE_CTAS 4     // resident 128-thread CTAs per SM the face pass is compiled for
+#endif
+#ifndef ADJ_CELL_CTAS
+#define ADJ_CELL_CTAS 8     // the same for the cell pass
+#endif
 template <int HEUN, int LIM>
-__global__ void __launch_bounds__(128, 4) adj_faces(AdjArgs a, long long nthr, double* FLx, double* FRx,
+__global__ void __launch_bounds__(128, ADJ_FACE_CTAS) adj_faces(AdjArgs a, long long nthr, double* FLx, double* FRx,
                                                     double* FLy, double* FRy) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, J;
@@ -255,7 +261,7 @@ __device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, 
 // 64 registers, eight 128-thread CTAs per SM: the pass waits on its neighbour loads, and
 // more loads in flight pay for the spills (measured, 4 x 256^2: 8 CTAs 10 % faster than 4)
 template <int HEUN, int LIM>
-__global__ void __launch_bounds__(128, 8) adj_cells(AdjArgs a, long long nthr, const double* FLx,
+__global__ void __launch_bounds__(128, ADJ_CELL_CTAS) adj_cells(AdjArgs a, long long nthr, const double* FLx,
                                                     const double* FRx, const double* FLy, const double* FRy) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, J;
