@@ -427,6 +427,7 @@ def main():
         stream.synchronize()
     attempts = s.attempts()
     launch = s.config()
+    launch["stage2_bulk_tensor_copies"] = s.bulk_copies()
     ms = e0.elapsed_time(e1)
     barrier()
     ms_max = ms

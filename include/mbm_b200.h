@@ -243,6 +243,15 @@ int mbm_shard_cfl(mbm_ctx *ctx);                      /* this rank's CFL of the 
 int mbm_shard_control(mbm_ctx *ctx, int *done);
 int mbm_shard_end(mbm_ctx *ctx, double *t, int *nsteps, int *nrej);
 
+/* No counterpart in the reference.  *on = 1 when the fast stage kernel's second Heun
+ * stage fills its shared-memory rows by bulk tensor copies (TMA: 3-D tensor maps over
+ * the context's TMP and relaxation layers, one copy of 32 columns x 9 moment planes per
+ * row, completion on mbarriers with bounded waits; a wait that runs out stops the case
+ * with MBM_ETIMEOUT); 0 when it uses per-lane asynchronous copies (bitwise mode, the
+ * environment variable MBM_TMA=0, or no tensor-map encoder in the driver: the reason is
+ * then in mbm_last_error). */
+int mbm_bulk_copies(mbm_ctx *ctx, int *on);
+
 /* Launch configuration in use: rows per warp work item (picked by the autotuner
  * when mbm_params.segment_rows is 0; the tuner's length may be fractional -- a strip
  * of n face rows gets ceil(n / length) equal segments -- and is reported rounded),

@@ -1,6 +1,7 @@
 // mbm_host.cu -- the C ABI (include/mbm_b200.h): context, block validation, the
 // resolved ghost map, the warp work table, the device-side step loop as a CUDA
 // graph with a conditional while node, and the layer transfers.
+#include <cuda.h>            // CUtensorMap and its encoder's types (the encoder is fetched at run time)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -88,6 +89,8 @@ struct mbm_ctx {
   long long layer_elems = 0;
   double* buf[3] = {nullptr, nullptr, nullptr};
   double* rlx = nullptr;            // fast arithmetic: the stage-1 relaxation term (a layer)
+  void* dtmap = nullptr;            // fast arithmetic: per block, tensor maps of TMP and rlx (stage-2 TMA)
+  std::string tma_note;             // why the stage-2 bulk tensor copies are off, if they are
   double* staging = nullptr;        // array-of-structs transfer buffer, one block
   GhostEntry* dghost = nullptr;
   int nghost = 0;
@@ -415,6 +418,9 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
     a.heun = heun;
     a.rlx = c->rlx;
     a.rlx_read = heun == 1 && rlx_read;
+    // bulk tensor copies: fast stage 2 on the context's own layers (the maps cover TMP
+    // and rlx; the adjoint's recomputation passes other buffers and keeps cp.async)
+    a.tmap = (c->fast && a.rlx_read && !bufs) ? c->dtmap : nullptr;
     cudaError_t e = c->fast ? fastmath::launch_stage(g.lim, a, g.grid[heun], st)
                             : bitwise::launch_stage(g.lim, a, g.grid[heun], st);
     if (e != cudaSuccess) return e;
@@ -539,6 +545,65 @@ static int autotune(mbm_ctx* c) {
     g_tune_cache[key] = best;
   }
   return set_segments(c, best);
+}
+
+// Tensor maps of the fast stage 2's bulk copies: for every block, its TMP layer and its
+// relaxation layer as 3-D tensors (column x pitch, row x nyp, moment plane x 9; strides
+// pitch and plane doubles), boxes of 32 columns x 1 row x 9 planes.  The TMA rules are
+// checked here, on the host, before any map exists: 16-byte aligned bases and strides, an
+// inner box of 256 bytes, and box origins (the strips' first columns, 28 k) on an even
+// column, i.e. a 16-byte boundary.  Rows and columns outside a block read zeros.  The
+// encoder comes from the driver at run time; without it, or with MBM_TMA=0, the stage
+// keeps its per-lane copies.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static_assert(sizeof(CUtensorMap) == TMAP_BYTES, "tensor map size");
+static_assert(STRIP % 2 == 0, "strip origins must stay on 16-byte boundaries");
+
+static void make_stage2_maps(mbm_ctx* c) {
+  const char* env = getenv("MBM_TMA");
+  if (env && atoi(env) == 0) { c->tma_note = "disabled by MBM_TMA=0"; return; }
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q{};
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn ||
+      q != cudaDriverEntryPointSuccess) {
+    cudaGetLastError();
+    c->tma_note = "cuTensorMapEncodeTiled unavailable";
+    return;
+  }
+  const EncodeTiledFn encode = (EncodeTiledFn)fn;
+  std::vector<CUtensorMap> maps((size_t)c->nblk * 2);
+  for (int b = 0; b < c->nblk; b++) {
+    const BlockDev& d = c->hblk[b];
+    double* base[2] = {c->buf[2] + d.off, c->rlx + d.off};
+    const cuuint64_t dims[3] = {(cuuint64_t)d.pitch, (cuuint64_t)d.nyp, (cuuint64_t)NV};
+    const cuuint64_t strides[2] = {(cuuint64_t)d.pitch * sizeof(double), (cuuint64_t)d.plane * sizeof(double)};
+    const cuuint32_t box[3] = {32, 1, (cuuint32_t)NV}, estr[3] = {1, 1, 1};
+    if (strides[0] % 16 || strides[1] % 16 || d.pitch < 1) { c->tma_note = "unaligned strides"; return; }
+    for (int k = 0; k < 2; k++) {
+      if ((uintptr_t)base[k] % 16) { c->tma_note = "unaligned layer"; return; }
+      if (encode(&maps[(size_t)b * 2 + k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base[k], dims, strides, box, estr,
+                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+        c->tma_note = "tensor map encoding failed";
+        return;
+      }
+    }
+  }
+  void* dm = nullptr;
+  if (cudaMalloc(&dm, maps.size() * sizeof(CUtensorMap)) != cudaSuccess) {
+    cudaGetLastError();
+    c->tma_note = "no memory for the tensor maps";
+    return;
+  }
+  if (cudaMemcpy(dm, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(dm);
+    c->tma_note = "tensor map copy failed";
+    return;
+  }
+  c->dtmap = dm;
 }
 
 // exchange plan of one rank of a case split over ranks by block (mbm_create_sharded)
@@ -672,6 +737,7 @@ static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vecto
   CKC(cudaMalloc(&c->staging, sizeof(double) * max_cells * (NV + 1)));   // layers, or 10 output fields
   CKC(cudaMalloc(&c->dblk, sizeof(BlockDev) * nblocks));
   CKC(cudaMemcpyAsync(c->dblk, c->hblk.data(), sizeof(BlockDev) * nblocks, cudaMemcpyHostToDevice, c->stream));
+  if (c->fast) make_stage2_maps(c);
 
   // ghost map in device element indices
   std::vector<GhostEntry> gm(res.size());
@@ -816,6 +882,7 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   if (c->graph) cudaGraphDestroy(c->graph);
   for (int l = 0; l < 3; l++) cudaFree(c->buf[l]);
   cudaFree(c->rlx);
+  cudaFree(c->dtmap);
   cudaFree(c->staging);
   cudaFree(c->dblk);
   cudaFree(c->dghost);
@@ -1088,6 +1155,7 @@ extern "C" int mbm_steps_batch_wait(mbm_ctx* c, double* t, int* nsteps, int* nre
     if (h.status) worst = h.status;
   }
   if (worst == 2) return fail(c, MBM_ENONFINITE, "a stage wrote NaN or infinity, or CFL or dt became non-finite");
+  if (worst == 3) return fail(c, MBM_ETIMEOUT, "a bounded device wait for a bulk copy ran out");
   if (worst == 5) return fail(c, MBM_ESTEPLIMIT, "step attempts exceeded max_attempts");
   return MBM_OK;
 }
@@ -1126,6 +1194,13 @@ extern "C" int mbm_config(mbm_ctx* c, int* segment_rows, int* work_items, int* c
   return MBM_OK;
 }
 
+extern "C" int mbm_bulk_copies(mbm_ctx* c, int* on) {
+  if (!c || !on) return fail(c, MBM_EINVAL, "mbm_bulk_copies: bad argument");
+  *on = c->dtmap != nullptr;
+  if (!c->dtmap && !c->tma_note.empty()) c->err = c->tma_note;
+  return MBM_OK;
+}
+
 extern "C" int mbm_attempts(mbm_ctx* c, int* attempts) {
   if (!c || !attempts) return fail(c, MBM_EINVAL, "mbm_attempts: bad argument");
   int a = 0;
@@ -1138,7 +1213,7 @@ extern "C" int mbm_case_status(mbm_ctx* c, int* status, int n) {
   if (!c || !status || n < 0 || n > c->ncase) return fail(c, MBM_EINVAL, "mbm_case_status: bad argument");
   for (int k = 0; k < n; k++) {
     const int s = c->hcase[k].status;
-    status[k] = s == 2 ? MBM_ENONFINITE : s == 5 ? MBM_ESTEPLIMIT : MBM_OK;
+    status[k] = s == 2 ? MBM_ENONFINITE : s == 3 ? MBM_ETIMEOUT : s == 5 ? MBM_ESTEPLIMIT : MBM_OK;
   }
   return MBM_OK;
 }
@@ -1757,6 +1832,7 @@ extern "C" int mbm_shard_end(mbm_ctx* c, double* t, int* nsteps, int* nrej) {
   if (nsteps) *nsteps = h.nstep;
   if (nrej) *nrej = h.nrej;
   if (h.status == 2) return fail(c, MBM_ENONFINITE, "a stage wrote NaN or infinity, or CFL or dt became non-finite");
+  if (h.status == 3) return fail(c, MBM_ETIMEOUT, "a bounded device wait for a bulk copy ran out");
   if (h.status == 5) return fail(c, MBM_ESTEPLIMIT, "step attempts exceeded max_attempts");
   return MBM_OK;
 }

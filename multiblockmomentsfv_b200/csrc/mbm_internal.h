@@ -77,7 +77,14 @@ struct StageArgs {
   // on the same Data0, ran just before)
   double* rlx;
   int rlx_read;
+  // fast arithmetic, stage 2 with rlx_read: 2 tensor maps (CUtensorMap, 128 bytes each)
+  // per block, over the TMP layer and the relaxation layer, 3-D (column, row, moment
+  // plane); not null: the window slots are filled by bulk tensor copies (TMA) instead
+  // of per-lane cp.async
+  const void* tmap;
 };
+
+constexpr int TMAP_BYTES = 128;   // sizeof(CUtensorMap)
 
 struct AdjArgs {       // one stage of the discrete adjoint (mbm_adjoint.cu)
   const BlockDev* blk;

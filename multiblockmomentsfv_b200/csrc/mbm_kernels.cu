@@ -79,7 +79,8 @@ __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __res
     cs.cfl_last = cfl;
     cs.attempts++;
     if (cs.nonfinite) {       // a stage wrote a NaN or infinity: stop before accepting it
-      cs.status = 2;          // MBM_ENONFINITE
+      // bit 2: a bounded wait for a bulk copy ran out (MBM_ETIMEOUT), else MBM_ENONFINITE
+      cs.status = (cs.nonfinite & 2) ? 3 : 2;
       cs.done = 1;
     } else if (cfl > cs.CFLmax) {
       cs.dt = dt * cs.CFLreg / cfl;

@@ -60,10 +60,56 @@ struct WarpWindow2 : WarpWindow1 {
   double Ua[NV][32];      // the moments of the next row
   double D0a[NV][32];     // Data0 (or its stored relaxation term) of the next update row
   double UJa[NV][32];     // the moments of the next update row
+  // completion barriers of the bulk tensor copies into Ua and into D0a + UJa; the
+  // padding keeps every slot of every warp's window on a 128-byte boundary
+  unsigned long long bar[2];
+  unsigned long long pad_[14];
 };
+static_assert(sizeof(WarpWindow2) % 128 == 0, "window slots must stay 128-byte aligned");
 template <int HEUN>
 using WarpWindow = typename std::conditional<
     HEUN == 1, WarpWindow2, typename std::conditional<MBM_FAST_ARITH != 0, WarpWindowR, WarpWindow1>::type>::type;
+
+// Bulk tensor copies (TMA) of the fast stage 2: one elected lane copies the nine moment
+// planes of 32 columns of one row (a 32 x 1 x 9 box of a 3-D tensor map over a layer of
+// one block: column, row, plane) into a window slot, completing on an mbarrier of the
+// warp; no multicast, the maps cover only this device's layers.  Every wait is bounded.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// false when the phase did not complete within the bound (a copy that never lands)
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  for (int i = 0; i < (1 << 20); i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_rows(void* dst, const void* map, int x, int y, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(0), "r"(smem_u32(bar))
+      : "memory");
+}
+// this thread's earlier shared-memory accesses ordered before later bulk copies
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+constexpr unsigned ROW_BOX_BYTES = NV * 32 * sizeof(double);   // one 32 x 1 x 9 box
 
 // per-thread asynchronous 8-byte copy global -> shared (cp.async), and its groups
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
@@ -81,12 +127,16 @@ constexpr int STAGE_WARPS = STAGE_CTA_WARPS;
 #define STAGE_MIN_CTAS 3   // CTAs per SM the register budget is sized for (168 registers)
 #endif
 
+// One work item.  tma: stage 2 fills its window slots by bulk tensor copies (warp-
+// uniform; ph holds the phase bits of the warp's two window barriers across items).
+// Returns false when a bounded wait on a copy ran out: the case is flagged (the
+// controller stops it with a timeout status) and the warp stops taking items.
 template <int HEUN, int LIM>
-__device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, const int lane,
-                                           WarpWindow<HEUN>& win) {
+__device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, const int lane,
+                                           WarpWindow<HEUN>& win, const bool tma, unsigned& ph) {
   const BlockDev B = a.blk[w.blk];
   const CaseDev& cs = a.cases[B.case_id];
-  if (cs.done) return;
+  if (cs.done) return true;
   const int cur = cs.cur;
   const double dt = cs.dt, Fx = cs.F;
   const Recip Kn(cs.Kn);
@@ -132,8 +182,37 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   // J+1 while it finishes row J (= r-2):
   // one group per fetch, committed even when empty, so that the groups alternate
   // U(r), D0(r-2), U(r+1), D0(r-1), ... and each wait leaves only the newest in flight
+  // bulk tensor copies: lane 0 issues each fetch after every lane has read the slot
+  // (__syncwarp, then the proxy fence); a fetch of a row outside the block completes
+  // its barrier phase with a plain arrive, so every fetch is matched by one wait
+  const char* maps = tma ? (const char*)a.tmap + (size_t)w.blk * 2 * TMAP_BYTES : nullptr;
+  const int tx0 = w.I0 - 1;        // tensor column of lane 0 (C + 1): 28 k, a multiple of 2 doubles
+  bool aborted = false;
+  int abort_k = -1;                // the barrier whose wait ran out
+  auto bar_wait = [&](int k) {     // wait for the phase of barrier k; false: ran out
+    if constexpr (HEUN == 1) {
+      const bool okw = __all_sync(0xffffffffu, mbar_wait(&win.bar[k], (ph >> k) & 1u));
+      ph ^= 1u << k;
+      if (!okw) abort_k = k;
+      return okw;
+    }
+    return true;
+  };
   auto u_fetch = [&](int rr) {
     if constexpr (HEUN == 1) {
+      if (tma) {
+        __syncwarp();
+        if (lane == 0) {
+          fence_proxy_async();
+          if (rr >= 0 && rr < nyp) {
+            mbar_expect_tx(&win.bar[0], ROW_BOX_BYTES);
+            tma_rows(win.Ua, maps, tx0, rr, &win.bar[0]);
+          } else {
+            mbar_arrive(&win.bar[0]);
+          }
+        }
+        return;
+      }
       if (col_in && rr >= 0 && rr < nyp) {
         const long long idx = (long long)rr * pitch + C + 1;
 #pragma unroll
@@ -144,6 +223,20 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
   };
   auto d0_fetch = [&](int Jn) {
     if constexpr (HEUN == 1) {
+      if (tma) {
+        __syncwarp();
+        if (lane == 0) {
+          fence_proxy_async();
+          if (Jn >= NG && Jn <= nyp - 1 - NG && Jn >= w.J0 && Jn < w.J1) {
+            mbar_expect_tx(&win.bar[1], 2 * ROW_BOX_BYTES);
+            tma_rows(win.D0a, maps + TMAP_BYTES, tx0, Jn, &win.bar[1]);
+            tma_rows(win.UJa, maps, tx0, Jn, &win.bar[1]);
+          } else {
+            mbar_arrive(&win.bar[1]);
+          }
+        }
+        return;
+      }
       if (col_out && Jn >= NG && Jn <= nyp - 1 - NG && Jn >= w.J0 && Jn < w.J1) {
         const long long idx = (long long)Jn * pitch + C + 1;
 #pragma unroll
@@ -176,7 +269,11 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
         if (okn) load_cell(in, plane, (long long)(r + 1) * pitch + C + 1, Un);
         else benign(Un);
       } else if constexpr (HEUN == 1) {
-        cp_async_wait_one();                 // this row's moments have landed
+        if (tma) {
+          if (!bar_wait(0)) { aborted = true; break; }
+        } else {
+          cp_async_wait_one();               // this row's moments have landed
+        }
         if (ok) {
 #pragma unroll
           for (int n = 0; n < NV; n++) U[n] = win.Ua[n][lane];
@@ -295,7 +392,13 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     }
     // (c) row J = r-2: x slope, x face C | C+1 (src/Main.c:346-347, 372-378), update
     const int J = r - 2;
-    if (HEUN == 1) cp_async_wait_one();     // this row's Data0 has landed
+    if (HEUN == 1) {                        // this row's Data0 and moments have landed
+      if (tma) {
+        if (!bar_wait(1)) { aborted = true; break; }
+      } else {
+        cp_async_wait_one();
+      }
+    }
     if (J >= w.J0 && J < w.J1) {
       double P0[NV], Sx[NV], lo[NV], hi[NV], F[NV];
       __syncwarp();   // the window row is read across lanes below (other lanes wrote it)
@@ -416,7 +519,27 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     d0_fetch(r - 1);                        // the next update row, into the slot row J has left
     s0 = s0 == 2 ? 0 : s0 + 1;
   }
-  if (HEUN == 1) cp_async_wait_all();       // nothing in flight past the work item
+  if constexpr (HEUN == 1) {                // nothing in flight past the work item
+    if (tma) {
+      if (aborted) {
+        // a copy did not land within the bound: flag the case, give the copies still in
+        // flight one more bounded wait (the phase that ran out, and the one fetch
+        // pending on the other barrier), and stop taking items
+        if (lane == 0) atomicOr(&a.cases[B.case_id].nonfinite, 2);
+        for (int k = 0; k < 2; k++) {
+          const unsigned par = (ph >> k) & 1u;
+          mbar_wait(&win.bar[k], k == abort_k ? par ^ 1u : par);
+        }
+        return false;
+      }
+      if (!bar_wait(0) || !bar_wait(1)) {
+        if (lane == 0) atomicOr(&a.cases[B.case_id].nonfinite, 2);
+        return false;
+      }
+    } else {
+      cp_async_wait_all();
+    }
+  }
 
   // per-block maxima; the values are >= 0 (or NaN, which never passes a '>' test
   // above), so their bit patterns order like the values
@@ -434,6 +557,7 @@ __device__ __forceinline__ void stage_item(const StageArgs& a, const Work w, con
     if (lamy > 0.0) atomicMax(slot + 1, (unsigned long long)__double_as_longlong(lamy));
     if (prod > 0.0) atomicMax(slot + 2, (unsigned long long)__double_as_longlong(prod));
   }
+  return true;
 }
 
 // Persistent grid (as many CTAs as fit on the SMs); every warp takes the next work
@@ -454,15 +578,32 @@ constexpr int stage_smem() { return (int)sizeof(WarpWindow<HEUN>) * STAGE_WARPS;
 #endif
 template <int HEUN, int LIM>
 __global__ void STAGE_BOUNDS stage_kernel(const StageArgs a) {
-  extern __shared__ __align__(16) unsigned char stage_shared[];
+  extern __shared__ __align__(128) unsigned char stage_shared[];
   WarpWindow<HEUN>* win = reinterpret_cast<WarpWindow<HEUN>*>(stage_shared);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool tma = false;
+  unsigned ph = 0;
+#if MBM_FAST_ARITH
+  if constexpr (HEUN == 1) {
+    // bulk tensor copies need 128-byte aligned slots (the window layout keeps them so
+    // from an aligned base; otherwise the per-lane copies serve)
+    tma = a.tmap != nullptr && (smem_u32(&win[warp]) & 127u) == 0;
+    if (tma) {
+      if (lane == 0) {
+        mbar_init(&win[warp].bar[0]);
+        mbar_init(&win[warp].bar[1]);
+        fence_mbar_init();
+      }
+      __syncwarp();
+    }
+  }
+#endif
   for (;;) {
     int w = 0;
     if (lane == 0) w = atomicAdd(a.queue, 1);
     w = __shfl_sync(0xffffffffu, w, 0);
     if (w >= a.nwork) break;
-    stage_item<HEUN, LIM>(a, a.work[w], lane, win[warp]);
+    if (!stage_item<HEUN, LIM>(a, a.work[w], lane, win[warp], tma, ph)) break;
   }
 }
 

@@ -175,6 +175,12 @@ class Solver:
         self._check(self.L.mbm_config(self.ctx, C.byref(a), C.byref(b), C.byref(c)))
         return {"segment_rows": a.value, "work_items": b.value, "ctas": c.value}
 
+    def bulk_copies(self) -> bool:
+        """Whether the fast stage 2 fills its rows by bulk tensor copies (TMA)."""
+        on = C.c_int(0)
+        self._check(self.L.mbm_bulk_copies(self.ctx, C.byref(on)))
+        return bool(on.value)
+
     def time_stage(self, heun: int, dt: float, reps: int = 10) -> float:
         """Mean device milliseconds of one stage-kernel launch (CUDA events)."""
         ms = C.c_double(0.0)

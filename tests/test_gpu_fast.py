@@ -181,3 +181,25 @@ def test_fast_reciprocal_and_root_within_one_ulp():
     print("fast reciprocal: max %.2f ulp, %.3f%% not correctly rounded; root: max %.2f ulp, %.3f%%" %
           (ulp_r.max(), 100 * np.mean(ulp_r > 0), ulp_q.max(), 100 * np.mean(ulp_q > 0)))
     assert ulp_r.max() <= 1.0 and ulp_q.max() <= 1.0
+
+
+@pytest.mark.parametrize("limiter", [bf.LIM_HARMONIC, bf.LIM_SUPERBEE])
+def test_bulk_tensor_copies_equal_per_lane_copies(limiter, monkeypatch):
+    """The fast stage 2 fills its shared-memory rows by bulk tensor copies (TMA) or, with
+    MBM_TMA=0, by per-lane asynchronous copies: the same bytes land either way, so the
+    runs agree bit for bit (states, steps, rejections); block sizes that leave partial
+    strips and rows exercise the copies that reach past a block's edge (zero fill)."""
+    cases = [H.quadrant_deck(n, Kn=0.01, limiter=limiter) for n in (37, 100)]
+    scn = sc.Scenario.seeded_quadrant(5)
+    for d in cases:
+        res = []
+        for tma in ("1", "0"):
+            monkeypatch.setenv("MBM_TMA", tma)
+            with sv.Solver(d, scn, mode="fast", show_every=0) as s:
+                assert s.bulk_copies() == (tma == "1"), _abi.lib().mbm_last_error(s.ctx)
+                s.initialise()
+                t, n, r = s.steps(0.0, 0.05)
+                res.append(((t, n, r), [s.download(sv.L_DATA, b) for b in range(len(d.blocks))]))
+        assert res[0][0] == res[1][0] and res[0][0][1] > 0
+        for b in range(len(d.blocks)):
+            H.assert_bitwise(res[0][1][b], res[1][1][b], f"block {b + 1}")
