@@ -44,31 +44,27 @@ __device__ __forceinline__ void load_cell(const double* __restrict__ base, long 
 
 // Rolling state of one warp, lane fastest (conflict-free 8-byte accesses): the
 // projected primitives of three consecutive rows, the lower state of the next
-// y face and the y flux of the face below the row being finished.  Stage 2 adds three
-// slots its asynchronous copies land in (stage 1 prefetches into registers); stage 1
-// in fast arithmetic keeps the relaxation term of the last three rows, which the
-// update of the row two iterations later reads from here, not from global memory.
+// y face and the y flux of the face below the row being finished.  Stage 2 adds two
+// slots its asynchronous copies land in (stage 1 prefetches into registers).  Measured
+// and dropped: stage 1 keeping its relaxation terms in a window ring instead of reading
+// them back from global memory (neutral to 5 % slower), and stage 2 copying the update
+// row's moments into a third slot (per-lane copies: 20 % slower than loading them).
 struct WarpWindow1 {
   double P[3][NV][32];
   double lo[NV][32];
   double G[NV][32];
 };
-struct WarpWindowR : WarpWindow1 {
-  double R[3][NV][32];    // relax<-1> of rows r-2 .. r (the ring of P)
-};
 struct WarpWindow2 : WarpWindow1 {
   double Ua[NV][32];      // the moments of the next row
   double D0a[NV][32];     // Data0 (or its stored relaxation term) of the next update row
-  double UJa[NV][32];     // the moments of the next update row
-  // completion barriers of the bulk tensor copies into Ua and into D0a + UJa; the
-  // padding keeps every slot of every warp's window on a 128-byte boundary
+  // completion barriers of the bulk tensor copies into Ua and into D0a; the padding
+  // keeps every slot of every warp's window on a 128-byte boundary
   unsigned long long bar[2];
   unsigned long long pad_[14];
 };
 static_assert(sizeof(WarpWindow2) % 128 == 0, "window slots must stay 128-byte aligned");
 template <int HEUN>
-using WarpWindow = typename std::conditional<
-    HEUN == 1, WarpWindow2, typename std::conditional<MBM_FAST_ARITH != 0, WarpWindowR, WarpWindow1>::type>::type;
+using WarpWindow = typename std::conditional<HEUN == 1, WarpWindow2, WarpWindow1>::type;
 
 // Bulk tensor copies (TMA) of the fast stage 2: one elected lane copies the nine moment
 // planes of 32 columns of one row (a 32 x 1 x 9 box of a 3-D tensor map over a layer of
@@ -144,9 +140,9 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
   const double* __restrict__ d0 = a.buf[phys_layer(a.sel_d0, cur)] + B.off;
   double* __restrict__ out = a.buf[phys_layer(a.sel_out, cur)] + B.off;
 #if MBM_FAST_ARITH
-  // the relaxation term of the stage-1 input: written by stage 1 at its row r (also
-  // into the window, where the update of that row two iterations later reads it);
-  // stage 2 reads it with rlx_read in place of forming it from Data0
+  // the relaxation term of the stage-1 input: written by stage 1 at its row r and read
+  // back (plain loads: written in this launch) by the update of that row two
+  // iterations later; stage 2 reads it with rlx_read in place of forming it from Data0
   double* __restrict__ rlx = a.rlx + B.off;
   const bool rlx_rd = HEUN == 1 && a.rlx_read;
   const double* __restrict__ d0src = rlx_rd ? rlx : d0;
@@ -178,8 +174,8 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
   // which stage 2, holding Data0 as well, cannot spare without spilling).
   constexpr bool PREFETCH = HEUN == 0;
   // Stage 2 copies, without registers, the moments of row r+1 into shared memory while
-  // it works on row r, and Data0 (or its relaxation term) and the moments of update row
-  // J+1 while it finishes row J (= r-2):
+  // it works on row r, and Data0 (or its relaxation term) of update row J+1 while it
+  // finishes row J (= r-2):
   // one group per fetch, committed even when empty, so that the groups alternate
   // U(r), D0(r-2), U(r+1), D0(r-1), ... and each wait leaves only the newest in flight
   // bulk tensor copies: lane 0 issues each fetch after every lane has read the slot
@@ -228,9 +224,8 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
         if (lane == 0) {
           fence_proxy_async();
           if (Jn >= NG && Jn <= nyp - 1 - NG && Jn >= w.J0 && Jn < w.J1) {
-            mbar_expect_tx(&win.bar[1], 2 * ROW_BOX_BYTES);
+            mbar_expect_tx(&win.bar[1], ROW_BOX_BYTES);
             tma_rows(win.D0a, maps + TMAP_BYTES, tx0, Jn, &win.bar[1]);
-            tma_rows(win.UJa, maps, tx0, Jn, &win.bar[1]);
           } else {
             mbar_arrive(&win.bar[1]);
           }
@@ -240,10 +235,7 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
       if (col_out && Jn >= NG && Jn <= nyp - 1 - NG && Jn >= w.J0 && Jn < w.J1) {
         const long long idx = (long long)Jn * pitch + C + 1;
 #pragma unroll
-        for (int n = 0; n < NV; n++) {
-          cp_async8(&win.D0a[n][lane], d0src + n * plane + idx);
-          cp_async8(&win.UJa[n][lane], in + n * plane + idx);
-        }
+        for (int n = 0; n < NV; n++) cp_async8(&win.D0a[n][lane], d0src + n * plane + idx);
       }
       cp_async_commit();
     }
@@ -300,7 +292,6 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
 #pragma unroll
           for (int n = 0; n < NV; n++) {
             rlx[n * plane + idx] = R0[n];
-            if constexpr (HEUN == 0) win.R[s0][n][lane] = R0[n];
           }
         }
         if (!(col_ring || r == 0 || r == nyp - 1)) {
@@ -456,11 +447,10 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
 #if MBM_FAST_ARITH
         const double g = dt * Fx;
         if constexpr (HEUN == 1) {
-#pragma unroll
-          for (int n = 0; n < NV; n++) U[n] = win.UJa[n][lane];
+          load_cell(in, plane, idx, U);
         } else {
 #pragma unroll
-          for (int n = 0; n < NV; n++) U[n] = win.R[sm2][n][lane];    // relax<-1> of this cell
+          for (int n = 0; n < NV; n++) U[n] = rlx[n * plane + idx];   // relax<-1> of this cell
         }
         // stage 1: relax<0> = the force push of relax<-1>; stage 2: relax<2> = the force
         // push of the moments (both the identity without a force)
@@ -471,12 +461,7 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
           for (int n = 0; n < NV; n++) R[n] = U[n];
         }
 #else
-        if constexpr (HEUN == 1) {
-#pragma unroll
-          for (int n = 0; n < NV; n++) U[n] = win.UJa[n][lane];
-        } else {
-          load_cell(in, plane, idx, U);
-        }
+        load_cell(in, plane, idx, U);
         primitive(U, Q);
         relax<2 * HEUN>(Q, R, dt, Kn, Fx);
 #endif
