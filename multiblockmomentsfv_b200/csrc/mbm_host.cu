@@ -139,7 +139,6 @@ struct mbm_ctx {
   double* adj_seg[2] = {nullptr};    // DATA states of a checkpoint segment (two: recomputation of
   double* adj_segT[2] = {nullptr};   //   the next one beside the reversal of this one); stage-1 states
   cudaStream_t adj_rstream = nullptr;   // the recomputation stream (low priority)
-  int adj_fwd_ctas = 0;                 // CTAs per SM of the recomputation's stage kernels (0: all that fit)
   cudaEvent_t adj_ready[2] = {nullptr}, adj_free[2] = {nullptr}, adj_start = nullptr;
   double* adj_dtlog = nullptr;
   double* adj_scal = nullptr;       // [0] dJ/dKn, [1] J
@@ -422,11 +421,8 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
     // bulk tensor copies: fast stage 2 on the context's own layers (the maps cover TMP
     // and rlx; the adjoint's recomputation passes other buffers and keeps cp.async)
     a.tmap = (c->fast && a.rlx_read && !bufs) ? c->dtmap : nullptr;
-    int grid = g.grid[heun];
-    if (bufs && c->adj_fwd_ctas > 0)    // the adjoint's recomputation (frozen_step)
-      grid = std::min(grid, c->nsm * std::min(c->adj_fwd_ctas, c->ctas_per_sm[heun]));
-    cudaError_t e = c->fast ? fastmath::launch_stage(g.lim, a, grid, st)
-                            : bitwise::launch_stage(g.lim, a, grid, st);
+    cudaError_t e = c->fast ? fastmath::launch_stage(g.lim, a, g.grid[heun], st)
+                            : bitwise::launch_stage(g.lim, a, g.grid[heun], st);
     if (e != cudaSuccess) return e;
   }
   for (int k = 1; k < ng; k++) {
@@ -1289,10 +1285,6 @@ static int adj_alloc(mbm_ctx* c, int nsteps, int every) {
   if (!c->adj_work_ready) {   // row-marching work: strips of ASTRIP columns x 32-row segments of the non-ring cells
     const char* env = getenv("MBM_ADJ_MARCH");
     c->adj_march = env && atoi(env) == 1;
-    // the recomputation's stage kernels on fewer CTAs per SM, so that the reversal's
-    // passes find room beside them (MBM_ADJ_FWD_CTAS; 0 or unset: every CTA that fits)
-    const char* fe = getenv("MBM_ADJ_FWD_CTAS");
-    c->adj_fwd_ctas = fe ? std::max(0, atoi(fe)) : 0;
     std::vector<Work> wl;
     for (int b = 0; b < c->nblk; b++) {
       const BlockDev& d = c->hblk[b];
