@@ -123,13 +123,16 @@ constexpr int STAGE_WARPS = STAGE_CTA_WARPS;
 #define STAGE_MIN_CTAS 3   // CTAs per SM the register budget is sized for (168 registers)
 #endif
 
-// One work item.  tma: stage 2 fills its window slots by bulk tensor copies (warp-
-// uniform; ph holds the phase bits of the warp's two window barriers across items).
+// One work item.  TMA (the fast stage 2 only): the instantiation that can fill its window
+// slots by bulk tensor copies; tma: whether it does (warp-uniform; ph holds the phase
+// bits of the warp's two window barriers across items).  The instantiation without it
+// carries only the per-lane copies: the unused branches alone cost 4 % of stage 2.
 // Returns false when a bounded wait on a copy ran out: the case is flagged (the
 // controller stops it with a timeout status) and the warp stops taking items.
-template <int HEUN, int LIM>
+template <int HEUN, int LIM, bool TMA>
 __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, const int lane,
-                                           WarpWindow<HEUN>& win, const bool tma, unsigned& ph) {
+                                           WarpWindow<HEUN>& win, const bool tma_on, unsigned& ph) {
+  const bool tma = TMA && tma_on;
   const BlockDev B = a.blk[w.blk];
   const CaseDev& cs = a.cases[B.case_id];
   if (cs.done) return true;
@@ -561,7 +564,7 @@ constexpr int stage_smem() { return (int)sizeof(WarpWindow<HEUN>) * STAGE_WARPS;
 #else
 #define STAGE_BOUNDS __launch_bounds__(32 * STAGE_WARPS, STAGE_MIN_CTAS)
 #endif
-template <int HEUN, int LIM>
+template <int HEUN, int LIM, bool TMA>
 __global__ void STAGE_BOUNDS stage_kernel(const StageArgs a) {
   extern __shared__ __align__(128) unsigned char stage_shared[];
   WarpWindow<HEUN>* win = reinterpret_cast<WarpWindow<HEUN>*>(stage_shared);
@@ -569,7 +572,7 @@ __global__ void STAGE_BOUNDS stage_kernel(const StageArgs a) {
   bool tma = false;
   unsigned ph = 0;
 #if MBM_FAST_ARITH
-  if constexpr (HEUN == 1) {
+  if constexpr (HEUN == 1 && TMA) {
     // bulk tensor copies need 128-byte aligned slots (the window layout keeps them so
     // from an aligned base; otherwise the per-lane copies serve)
     tma = a.tmap != nullptr && (smem_u32(&win[warp]) & 127u) == 0;
@@ -588,13 +591,17 @@ __global__ void STAGE_BOUNDS stage_kernel(const StageArgs a) {
     if (lane == 0) w = atomicAdd(a.queue, 1);
     w = __shfl_sync(0xffffffffu, w, 0);
     if (w >= a.nwork) break;
-    if (!stage_item<HEUN, LIM>(a, a.work[w], lane, win[warp], tma, ph)) break;
+    if (!stage_item<HEUN, LIM, TMA>(a, a.work[w], lane, win[warp], tma, ph)) break;
   }
 }
 
 template <int HEUN, int LIM>
 static void smem_attr() {
-  cudaFuncSetAttribute(stage_kernel<HEUN, LIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_smem<HEUN>());
+  cudaFuncSetAttribute(stage_kernel<HEUN, LIM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       stage_smem<HEUN>());
+  if constexpr (HEUN == 1 && MBM_FAST_ARITH != 0)
+    cudaFuncSetAttribute(stage_kernel<HEUN, LIM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         stage_smem<HEUN>());
 }
 
 // called at context creation (the device current), before any launch or graph capture:
@@ -616,28 +623,32 @@ int stage_ctas_per_sm(int heun) {
   }
   int n = 0;
   if (heun)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<1, 4>, 32 * STAGE_WARPS, stage_smem<1>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<1, 4, false>, 32 * STAGE_WARPS, stage_smem<1>());
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<0, 4>, 32 * STAGE_WARPS, stage_smem<0>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<0, 4, false>, 32 * STAGE_WARPS, stage_smem<0>());
   return n > 0 ? n : 1;
 }
 
 int stage_cta_warps() { return STAGE_WARPS; }
 
-template <int HEUN>
+template <int HEUN, bool TMA>
 static cudaError_t launch_stage_lim(int lim, const StageArgs& a, int grid, cudaStream_t s) {
   switch (lim) {
-    case 0: stage_kernel<HEUN, 0><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
-    case 1: stage_kernel<HEUN, 1><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
-    case 2: stage_kernel<HEUN, 2><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
-    case 3: stage_kernel<HEUN, 3><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
-    default: stage_kernel<HEUN, 4><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
+    case 0: stage_kernel<HEUN, 0, TMA><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
+    case 1: stage_kernel<HEUN, 1, TMA><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
+    case 2: stage_kernel<HEUN, 2, TMA><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
+    case 3: stage_kernel<HEUN, 3, TMA><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
+    default: stage_kernel<HEUN, 4, TMA><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_stage(int lim, const StageArgs& a, int grid, cudaStream_t s) {
-  return a.heun ? launch_stage_lim<1>(lim, a, grid, s) : launch_stage_lim<0>(lim, a, grid, s);
+  if (!a.heun) return launch_stage_lim<0, false>(lim, a, grid, s);
+#if MBM_FAST_ARITH
+  if (a.tmap) return launch_stage_lim<1, true>(lim, a, grid, s);
+#endif
+  return launch_stage_lim<1, false>(lim, a, grid, s);
 }
 
 }  // namespace MBM_ARITH
