@@ -247,9 +247,10 @@ int mbm_shard_end(mbm_ctx *ctx, double *t, int *nsteps, int *nrej);
  * stage fills its shared-memory rows by bulk tensor copies (TMA: 3-D tensor maps over
  * the context's TMP and relaxation layers, one copy of 32 columns x 9 moment planes per
  * row, completion on mbarriers with bounded waits; a wait that runs out stops the case
- * with MBM_ETIMEOUT); 0 when it uses per-lane asynchronous copies (bitwise mode, the
- * environment variable MBM_TMA=0, or no tensor-map encoder in the driver: the reason is
- * then in mbm_last_error). */
+ * with MBM_ETIMEOUT); 0 when it uses per-lane asynchronous copies, the default (the
+ * environment variable MBM_TMA=1 at context creation selects the bulk copies, which
+ * measured slower on this kernel; bitwise mode and a driver without the tensor-map
+ * encoder always use the per-lane copies; the reason is then in mbm_last_error). */
 int mbm_bulk_copies(mbm_ctx *ctx, int *on);
 
 /* Launch configuration in use: rows per warp work item (picked by the autotuner
