@@ -131,7 +131,8 @@ constexpr int STAGE_WARPS = STAGE_CTA_WARPS;
 // controller stops it with a timeout status) and the warp stops taking items.
 template <int HEUN, int LIM, bool TMA>
 __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, const int lane,
-                                           WarpWindow<HEUN>& win, const bool tma_on, unsigned& ph) {
+                                           WarpWindow<HEUN>& win, const bool tma_on, unsigned& ph,
+                                           bool& drop) {
   const bool tma = TMA && tma_on;
   const BlockDev B = a.blk[w.blk];
   const CaseDev& cs = a.cases[B.case_id];
@@ -203,13 +204,16 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
         __syncwarp();
         if (lane == 0) {
           fence_proxy_async();
-          if (rr >= 0 && rr < nyp) {
+          if (drop) {
+            // failure-detection test: neither copy nor arrive, the phase never completes
+          } else if (rr >= 0 && rr < nyp) {
             mbar_expect_tx(&win.bar[0], ROW_BOX_BYTES);
             tma_rows(win.Ua, maps, tx0, rr, &win.bar[0]);
           } else {
             mbar_arrive(&win.bar[0]);
           }
         }
+        drop = false;
         return;
       }
       if (col_in && rr >= 0 && rr < nyp) {
@@ -569,13 +573,14 @@ __global__ void STAGE_BOUNDS stage_kernel(const StageArgs a) {
   extern __shared__ __align__(128) unsigned char stage_shared[];
   WarpWindow<HEUN>* win = reinterpret_cast<WarpWindow<HEUN>*>(stage_shared);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  bool tma = false;
+  bool tma = false, drop = false;
   unsigned ph = 0;
 #if MBM_FAST_ARITH
   if constexpr (HEUN == 1 && TMA) {
     // bulk tensor copies need 128-byte aligned slots (the window layout keeps them so
     // from an aligned base; otherwise the per-lane copies serve)
     tma = a.tmap != nullptr && (smem_u32(&win[warp]) & 127u) == 0;
+    drop = tma && a.tma_drop && blockIdx.x == 0 && warp == 0;
     if (tma) {
       if (lane == 0) {
         mbar_init(&win[warp].bar[0]);
@@ -591,7 +596,7 @@ __global__ void STAGE_BOUNDS stage_kernel(const StageArgs a) {
     if (lane == 0) w = atomicAdd(a.queue, 1);
     w = __shfl_sync(0xffffffffu, w, 0);
     if (w >= a.nwork) break;
-    if (!stage_item<HEUN, LIM, TMA>(a, a.work[w], lane, win[warp], tma, ph)) break;
+    if (!stage_item<HEUN, LIM, TMA>(a, a.work[w], lane, win[warp], tma, ph, drop)) break;
   }
 }
 

@@ -9,6 +9,7 @@ import pytest
 import helpers as H
 from multiblockmomentsfv_b200 import _abi, output, solver
 from multiblockmomentsfv_b200 import scenario as sc
+from multiblockmomentsfv_b200 import solver as sv
 
 pytestmark = pytest.mark.gpu
 
@@ -129,3 +130,34 @@ def test_cli_matches_the_reference_binary(tmp_path):
     assert r2.returncode == 0
     ok, mx, msg = output.compare(str(tmp_path / "cli" / got[0]), str(tmp_path / "ref" / got[0]), 0.0, 0.0)
     assert ok and mx == 0.0, msg
+
+
+def test_bulk_copy_wait_that_runs_out_stops_the_case(monkeypatch):
+    """Failure detection of the bulk tensor copies (MBM_TMA=1): every wait on a copy's
+    mbarrier is bounded.  A test hook (MBM_TMA_TEST_DROP=1, one launch only) makes one warp
+    withhold its first copy, so that its wait runs out: the warp flags the case and stops,
+    the controller stops the case before accepting the attempt, and the call returns
+    MBM_ETIMEOUT with DATA untouched.  The context stays usable: the next call runs and
+    gives the bits of a run without the hook."""
+    monkeypatch.setenv("MBM_TMA", "1")
+    monkeypatch.setenv("MBM_AUTOTUNE", "0")       # no tuning launches before the step loop
+    d = H.quadrant_deck(64, Kn=0.01, limiter=4)
+    scn = sc.Scenario.seeded_quadrant(9)
+    with sv.Solver(d, scn, mode="fast", show_every=0) as clean:
+        clean.initialise()
+        ref = clean.steps(0.0, 0.02)
+        ref_layers = [clean.download(sv.L_DATA, b) for b in range(len(d.blocks))]
+    monkeypatch.setenv("MBM_TMA_TEST_DROP", "1")
+    with sv.Solver(d, scn, mode="fast", show_every=0) as s:
+        assert s.bulk_copies()
+        s.initialise()
+        start = [s.download(sv.L_DATA, b) for b in range(len(d.blocks))]
+        with pytest.raises(_abi.MBMError) as e:
+            s.steps(0.0, 0.02)
+        assert e.value.status == _abi.MBM_ETIMEOUT
+        for b in range(len(d.blocks)):
+            H.assert_bitwise(s.download(sv.L_DATA, b), start[b], f"block {b + 1} after the stopped attempt")
+        s.initialise()
+        assert s.steps(0.0, 0.02) == ref
+        for b in range(len(d.blocks)):
+            H.assert_bitwise(s.download(sv.L_DATA, b), ref_layers[b], f"block {b + 1}")
