@@ -80,19 +80,30 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned
 __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
+// one test of the phase; the thread may be suspended up to 20 us while it is incomplete
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
   unsigned done;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
       : "memory");
   return done != 0;
 }
-// false when the phase did not complete within the bound (a copy that never lands)
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// false when the phase did not complete within 0.25 s of device time (a copy that never
+// lands); at most 65,536 tests of at most 20 us each, should the timer not advance
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
-  for (int i = 0; i < (1 << 20); i++)
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (int i = 0; i < (1 << 16); i++) {
     if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > 250000000ull) return false;
+  }
   return false;
 }
 __device__ __forceinline__ void tma_rows(void* dst, const void* map, int x, int y, unsigned long long* bar) {
