@@ -119,6 +119,17 @@ int mbm_download(mbm_ctx *ctx, int layer, int block, double *cells);
  * doubles, the bytes the reference writes to its .dat file. */
 int mbm_output_fields(mbm_ctx *ctx, int block, int single, void *out);
 
+/* LoadData (src/Mesh.c:198-283) for one block, on the device: `payload` (host) is the
+ * block's zone of a result file as stored -- (nx+2)*(ny+2) points of the interior plus
+ * one ghost ring, x outer / y inner, the 10 fields rho vx vy T p Pxx Pxy Pyy qx qy
+ * fastest, float (single = 1) or double -- and becomes the moments of L_DATA; every other
+ * cell of the block becomes zero, as in the reference's main before its SetBoundary
+ * (call mbm_set_boundary next).  faithful = 0 keeps the reference's mapping (the stored
+ * p goes where theta belongs, P_ij where T_ij belongs), bit for bit; faithful = 1 maps
+ * the fields to the state they were written from (theta = T, T_ij = P_ij / rho).  Only
+ * the payload crosses to the device. */
+int mbm_load_fields(mbm_ctx *ctx, int block, int single, const void *payload, int faithful);
+
 /* The same payload formed now (from DATA as it is) into device memory the context
  * keeps per block, and copied to `host` (page-locked, e.g. from mbm_host_alloc) on a
  * stream of its own, so that the copy runs beside the next step loop; mbm_output_wait

@@ -86,6 +86,19 @@ def load_restart(deck: bf.Deck, path: str, faithful: bool = False):
     return layers
 
 
+def restart_payloads(deck: bf.Deck, path: str, faithful: bool = False):
+    """The zones LoadData reads (src/Mesh.c:198-283) as stored, in the file's precision:
+    the first len(blocks) zones (the t = 0 level of a multi-level file), or with faithful
+    the last level; for mbm_load_fields, which forms the moments on the device."""
+    zones, _ = out.read(path, keep_dtype=True)
+    nb = len(deck.blocks)
+    sel = zones[len(zones) - nb:] if faithful else zones[:nb]
+    for b, z in zip(deck.blocks, sel):
+        if z["values"].shape != ((b.nx + 2) * (b.ny + 2), 10):
+            raise ValueError("restart file zone %d does not match block %d" % (z["block"], b.block_id))
+    return [z["values"] for z in sel]
+
+
 def main(argv=None) -> int:
     argv = sys.argv if argv is None else argv
     if "-h" in argv[1:] or "--help" in argv[1:]:
@@ -106,9 +119,10 @@ def main(argv=None) -> int:
     print("\n Running: Kn = %.4g, R13 = %g, CFL = %.2f, limiter = %s, BlockFile = \"%s\"" %
           (deck.Kn, deck.R13, deck.CFL, bf.limiter_name(deck.limiter), _arg(argv, "-bfile", "blockfile.txt")))
     sfile = _arg(argv, "-sfile")
-    initial = load_restart(deck, sfile, faithful="-restart-faithful" in argv) if sfile else None
+    faithful = "-restart-faithful" in argv
+    restart = (restart_payloads(deck, sfile, faithful), faithful) if sfile else None
     mode = "fast" if "-fast" in argv else "exact"
-    sv.run(deck, scn, out_dir, single=single, device=device, verbose=True, mode=mode, initial=initial)
+    sv.run(deck, scn, out_dir, single=single, device=device, verbose=True, mode=mode, restart=restart)
     return 0
 
 

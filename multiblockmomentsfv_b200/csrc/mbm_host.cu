@@ -57,6 +57,8 @@ cudaError_t launch_stage_cfl(const BlockDev* blk, int nblk, const CaseDev* cases
                              unsigned long long* lam, int stage, double* out, cudaStream_t s);
 cudaError_t launch_output_fields(const double* src, int nxp, int nyp, int pitch, long long plane, int single,
                                  void* dst, cudaStream_t s);
+cudaError_t launch_fields_to_planes(const void* src, int single, int faithful, int nxp, int nyp, int pitch,
+                                    long long plane, double* dst, cudaStream_t s);
 cudaError_t launch_aos_to_planes(const double* aos, double* dst, int nxp, int nyp, int pitch,
                                  long long plane, cudaStream_t s);
 cudaError_t launch_planes_to_aos(const double* src, double* aos, int nxp, int nyp, int pitch,
@@ -967,6 +969,19 @@ extern "C" int mbm_download(mbm_ctx* c, int layer, int block, double* cells) {
   const BlockDev& d = c->hblk[block];
   CK(launch_planes_to_aos(c->buf[phys_of(c, layer, block)] + d.off, c->staging, d.nxp, d.nyp, d.pitch, d.plane, c->stream));
   CK(cudaMemcpyAsync(cells, c->staging, sizeof(double) * d.nxp * d.nyp * NV, cudaMemcpyDeviceToHost, c->stream));
+  return wait_stream(c);
+}
+
+extern "C" int mbm_load_fields(mbm_ctx* c, int block, int single, const void* payload, int faithful) {
+  if (!c || !payload || block < 0 || block >= c->nblk || (single != 0 && single != 1) ||
+      (faithful != 0 && faithful != 1))
+    return fail(c, MBM_EINVAL, "mbm_load_fields: bad argument");
+  CK(cudaSetDevice(c->device));
+  const BlockDev& d = c->hblk[block];
+  const size_t bytes = (size_t)(d.nxp - 4) * (d.nyp - 4) * 10 * (single ? sizeof(float) : sizeof(double));
+  CK(cudaMemcpyAsync(c->staging, payload, bytes, cudaMemcpyHostToDevice, c->stream));
+  CK(launch_fields_to_planes(c->staging, single, faithful, d.nxp, d.nyp, d.pitch, d.plane,
+                             c->buf[phys_of(c, MBM_L_DATA, block)] + d.off, c->stream));
   return wait_stream(c);
 }
 

@@ -196,6 +196,65 @@ cudaError_t launch_output_fields(const double* src, int nxp, int nyp, int pitch,
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ restart load --
+// LoadData on the device (src/Mesh.c:198-283): one block's zone of a result file, as
+// stored (the interior plus one ghost ring, x outer / y inner, the 10 fields rho vx vy T
+// p Pxx Pxy Pyy qx qy fastest; float widened to double, as the reference reads a
+// Float32 file), becomes the moments of L_DATA; every other cell of the block is zero, as
+// the reference's main leaves it before SetBoundary.  The reference's mapping (faithful =
+// 0) puts the stored p where theta belongs and P_ij where T_ij belongs (src/Mesh.c:
+// 263-273); faithful = 1 maps the fields to the state they were written from
+// (theta = T, T_ij = P_ij / rho).  Conservative keeps the reference's expression order
+// (bitwise instantiation), so the moments equal the reference's LoadData bit for bit.
+__global__ void fields_to_planes(const void* __restrict__ src, int single, int faithful, int nxp, int nyp,
+                                 int pitch, long long plane, double* __restrict__ dst) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (long long)nxp * nyp) return;
+  const int J = (int)(k / nxp), I = (int)(k - (long long)J * nxp);
+  double U[NV];
+  if (I >= 2 && I <= nxp - 3 && J >= 2 && J <= nyp - 3) {
+    const long long p = (long long)(I - 2) * (nyp - 4) + (J - 2);
+    double v[10];
+    if (single) {
+#pragma unroll
+      for (int m = 0; m < 10; m++) v[m] = (double)((const float*)src)[p * 10 + m];
+    } else {
+#pragma unroll
+      for (int m = 0; m < 10; m++) v[m] = ((const double*)src)[p * 10 + m];
+    }
+    double P[NV];
+    P[0] = v[0];
+    P[1] = v[1];
+    P[2] = v[2];
+    if (faithful) {
+      P[3] = v[3];
+      P[4] = v[5] / v[0];
+      P[5] = v[6] / v[0];
+      P[6] = v[7] / v[0];
+    } else {
+      P[3] = v[4];
+      P[4] = v[5];
+      P[5] = v[6];
+      P[6] = v[7];
+    }
+    P[7] = v[8];
+    P[8] = v[9];
+    conservative(P, U);
+  } else {
+#pragma unroll
+    for (int m = 0; m < NV; m++) U[m] = 0.0;
+  }
+#pragma unroll
+  for (int m = 0; m < NV; m++) dst[m * plane + (long long)J * pitch + I + 1] = U[m];
+}
+
+cudaError_t launch_fields_to_planes(const void* src, int single, int faithful, int nxp, int nyp, int pitch,
+                                    long long plane, double* dst, cudaStream_t s) {
+  const long long n = (long long)nxp * nyp;
+  fields_to_planes<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(src, single, faithful, nxp, nyp, pitch, plane, dst);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ transposes --
 // host layout (cells x 9, x fastest, ghosts included) <-> device planes
 __global__ void aos_to_planes(const double* __restrict__ aos, double* __restrict__ dst, int nxp,

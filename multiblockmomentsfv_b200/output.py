@@ -163,9 +163,10 @@ def companion(path: str) -> Tuple[str, str]:
     return base + ".hdr", base + ".dat"
 
 
-def read(path: str):
+def read(path: str, keep_dtype: bool = False):
     """Read a result pair: returns (zones, precision) where zones is a list of
-    dicts with block, I, J, time and values (I*J, 10) as float64."""
+    dicts with block, I, J, time and values (I*J, 10) as float64 (keep_dtype: in the
+    file's precision, float32 for Float32 files)."""
     hdr, dat = companion(path)
     prec = "Float64"
     zones = []
@@ -185,7 +186,8 @@ def read(path: str):
     raw = np.fromfile(dat, dtype=np.uint8)
     for z in zones:
         n = z["nvars"] * z["I"] * z["J"]
-        z["values"] = raw[z["offset"]:z["offset"] + n * dt.itemsize].view(dt).astype(np.float64).reshape(-1, z["nvars"])
+        v = raw[z["offset"]:z["offset"] + n * dt.itemsize].view(dt)
+        z["values"] = (v.copy() if keep_dtype else v.astype(np.float64)).reshape(-1, z["nvars"])
     return zones, prec
 
 

@@ -89,6 +89,16 @@ class Solver:
     def layers(self, layer: int = L_DATA) -> List[np.ndarray]:
         return [self.download(layer, b) for b in range(len(self.deck.blocks))]
 
+    def load_fields(self, b: int, payload: np.ndarray, faithful: bool = False) -> None:
+        """LoadData of block b on the device (mbm_load_fields): payload is the block's zone
+        of a result file as stored, ((nx+2)*(ny+2), 10), float32 or float64."""
+        blk = self.deck.blocks[b]
+        p = np.ascontiguousarray(payload)
+        if p.dtype not in (np.float32, np.float64) or p.size != (blk.nx + 2) * (blk.ny + 2) * 10:
+            raise ValueError("payload has the wrong type or size")
+        self._check(self.L.mbm_load_fields(self.ctx, b, int(p.dtype == np.float32), p.ctypes.data_as(C.c_void_p),
+                                           int(bool(faithful))))
+
     def output_fields(self, b: int, single: bool = True) -> np.ndarray:
         """Output's payload of block b computed on the device: ((nx+2)*(ny+2), 10)."""
         blk = self.deck.blocks[b]
@@ -368,17 +378,23 @@ class PinnedArray:
 
 def run(deck: bf.Deck, scenario: sc.Scenario, out_dir: str, single: bool = True, device: int = 0,
         verbose: bool = True, show_every: int = 20, mode: str = "exact", overlap: bool = True,
-        initial: Optional[Sequence[np.ndarray]] = None):
+        initial: Optional[Sequence[np.ndarray]] = None, restart=None):
     """The reference's main() loop on the device: initial state and output at t=0,
     then Steps + Output per output time (src/Main.c:138-156).  Returns (writer, steps).
     overlap: each interval's output is formed on the device right after the interval,
     copied to the host beside the next interval and written to the files while the
-    GPU steps on (same files as without).  initial: L_DATA layers to start from (a
-    restart) instead of the scenario's initial state."""
+    GPU steps on (same files as without).  initial: L_DATA layers to start from instead
+    of the scenario's initial state; restart: (per-block payloads as stored in a result
+    file, faithful) to start from a restart, loaded on the device (mbm_load_fields)."""
     w = out.Writer(out_dir, deck, scenario.type_name, single)
     ft = np.float32 if single else np.float64
     with Solver(deck, scenario, device=device, show_every=show_every, mode=mode) as s:
-        if initial is not None:
+        if restart is not None:
+            payloads, faithful = restart
+            for b, p in enumerate(payloads):
+                s.load_fields(b, p, faithful)
+            s.set_boundary(L_DATA, 0.0)
+        elif initial is not None:
             for b, U in enumerate(initial):
                 s.upload(L_DATA, b, U)
             s.set_boundary(L_DATA, 0.0)

@@ -132,6 +132,62 @@ def test_cli_matches_the_reference_binary(tmp_path):
     assert ok and mx == 0.0, msg
 
 
+@pytest.mark.parametrize("single", [False, True])
+@pytest.mark.parametrize("faithful", [False, True])
+def test_device_restart_load_equals_host_loaddata(tmp_path, single, faithful):
+    """mbm_load_fields (LoadData on the device) against the host restart loader, which
+    equals the reference's own LoadData bit for bit (tests/test_restart.py): every cell of
+    L_DATA, both mappings, both payload precisions, on a two-level file."""
+    from multiblockmomentsfv_b200 import __main__ as cli
+    rng = np.random.default_rng(21 + 2 * single + faithful)
+    d = H.deck("Lshape")
+    lv = [[H.random_layer(rng, b) for b in d.blocks] for _ in range(2)]
+    w = output.Writer(str(tmp_path), d, "Riemann2D", single=single)
+    w.write(lv[0], 0.0, -1)
+    w.write(lv[1], 0.1, 5)
+    want = cli.load_restart(d, w.base, faithful=faithful)
+    payloads = cli.restart_payloads(d, w.base, faithful=faithful)
+    assert all(p.dtype == (np.float32 if single else np.float64) for p in payloads)
+    with sv.Solver(d, sc.Scenario.named("riemann2d")) as s:
+        for b in range(len(d.blocks)):
+            s.upload(sv.L_DATA, b, np.full((d.blocks[b].nyp, d.blocks[b].nxp, 9), 7.0))   # overwritten
+            s.load_fields(b, payloads[b], faithful)
+        for b in range(len(d.blocks)):
+            H.assert_bitwise(s.download(sv.L_DATA, b), want[b], f"block {b + 1}")
+
+
+def test_cli_restart_matches_the_reference_binary(tmp_path):
+    """-sfile through the Python mirror of main (the restart loaded on the device) and
+    through the reference binary (its own LoadData, CPU steps): identical files."""
+    import subprocess
+    import sys
+    ref = os.path.join(H.HERE, "..", "oracle", "_ref", "moments")
+    if not os.path.exists(ref):
+        pytest.skip("reference binary not built (make -C oracle ref)")
+    env = dict(os.environ, MBM_SCENARIO="riemann2d", OMP_NUM_THREADS="1")
+    text = open(os.path.join(H.DECKS, "squareSmall.txt")).read().splitlines()
+    def deck(t):
+        p = tmp_path / ("deck_%s.txt" % t)
+        p.write_text("\n".join(("t_list = " + t) if l.strip().startswith("t_list") else
+                                ("dt_out = 0" if l.strip().startswith("dt_out") else l) for l in text) + "\n")
+        return str(p)
+    r = subprocess.run([ref, "-bfile", deck("0.05"), "-out", str(tmp_path / "start"), "-double"], env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0
+    start = str(tmp_path / "start" / [f for f in os.listdir(tmp_path / "start") if f.endswith(".hdr")][0])
+    r1 = subprocess.run([sys.executable, "-m", "multiblockmomentsfv_b200", "-bfile", deck("0.1"), "-out",
+                         str(tmp_path / "cli"), "-double", "-sfile", start], capture_output=True, text=True,
+                        timeout=600, cwd=os.path.join(H.HERE, ".."))
+    assert r1.returncode == 0, r1.stderr[-2000:]
+    r2 = subprocess.run([ref, "-bfile", deck("0.1"), "-out", str(tmp_path / "ref"), "-double", "-sfile", start],
+                        env=env, capture_output=True, text=True, timeout=600)
+    assert r2.returncode == 0
+    got = [f for f in os.listdir(tmp_path / "cli") if f.endswith(".hdr")]
+    assert got == [f for f in os.listdir(tmp_path / "ref") if f.endswith(".hdr")]
+    ok, mx, msg = output.compare(str(tmp_path / "cli" / got[0]), str(tmp_path / "ref" / got[0]), 0.0, 0.0)
+    assert ok and mx == 0.0, msg
+
+
 def test_bulk_copy_wait_that_runs_out_stops_the_case(monkeypatch):
     """Failure detection of the bulk tensor copies (MBM_TMA=1): every wait on a copy's
     mbarrier is bounded.  A test hook (MBM_TMA_TEST_DROP=1, one launch only) makes one warp

@@ -90,3 +90,22 @@ def test_default_restart_equals_reference_loaddata(tmp_path, deck, single):
         got = cli.load_restart(d, name)
         for b in range(len(d.blocks)):
             H.assert_bitwise(got[b], ref[b], f"{deck} block {b + 1} ({name[-4:]})")
+
+
+@pytest.mark.parametrize("single", [False, True])
+def test_restart_payloads_as_stored(tmp_path, single):
+    """The zones the device loader receives (cli.restart_payloads): the file's values in
+    the file's precision, the first level by default and the last with faithful."""
+    d = H.deck("squareSmall")
+    lv = _levels(d, 9 + single)
+    w = output.Writer(str(tmp_path), d, "Riemann2D", single=single)
+    w.write(lv[0], 0.0, -1)
+    w.write(lv[1], 0.1, 5)
+    zones, _ = output.read(w.base)
+    nb = len(d.blocks)
+    for faithful, sel in ((False, zones[:nb]), (True, zones[nb:])):
+        got = cli.restart_payloads(d, w.base, faithful=faithful)
+        for b, (p, z) in enumerate(zip(got, sel)):
+            assert p.dtype == (np.float32 if single else np.float64)
+            assert p.shape == ((d.blocks[b].nx + 2) * (d.blocks[b].ny + 2), 10)
+            H.assert_bitwise(p.astype(np.float64), z["values"], f"block {b + 1}")
