@@ -93,7 +93,7 @@ struct mbm_ctx {
   double* rlx = nullptr;            // fast arithmetic: the stage-1 relaxation term (a layer)
   void* dtmap = nullptr;            // fast arithmetic: per block, tensor maps of TMP and rlx (stage-2 TMA)
   std::string tma_note;             // why the stage-2 bulk tensor copies are off, if they are
-  int tma_drop = 0;                 // failure-detection test: the next bulk-copy launch withholds one copy
+  int* dtma_drop = nullptr;         // failure-detection test: device flag, the next bulk-copy launch withholds one copy
   double* staging = nullptr;        // array-of-structs transfer buffer, one block
   GhostEntry* dghost = nullptr;
   int nghost = 0;
@@ -424,10 +424,7 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
     // bulk tensor copies: fast stage 2 on the context's own layers (the maps cover TMP
     // and rlx; the adjoint's recomputation passes other buffers and keeps cp.async)
     a.tmap = (c->fast && a.rlx_read && !bufs) ? c->dtmap : nullptr;
-    if (a.tmap && c->tma_drop) {       // one launch only: the context stays usable
-      a.tma_drop = 1;
-      c->tma_drop = 0;
-    }
+    if (a.tmap) a.tma_drop = c->dtma_drop;   // consumed on the device by the first launch
     cudaError_t e = c->fast ? fastmath::launch_stage(g.lim, a, g.grid[heun], st)
                             : bitwise::launch_stage(g.lim, a, g.grid[heun], st);
     if (e != cudaSuccess) return e;
@@ -616,7 +613,15 @@ static void make_stage2_maps(mbm_ctx* c) {
   // failure-detection test hook: the first bulk-copy launch of this context withholds one
   // copy, so that a bounded wait runs out and the case stops with MBM_ETIMEOUT
   const char* drop = getenv("MBM_TMA_TEST_DROP");
-  c->tma_drop = drop && atoi(drop) == 1;
+  if (drop && atoi(drop) == 1) {
+    const int one = 1;
+    if (cudaMalloc(&c->dtma_drop, sizeof(int)) != cudaSuccess ||
+        cudaMemcpy(c->dtma_drop, &one, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(c->dtma_drop);
+      c->dtma_drop = nullptr;
+    }
+  }
 }
 
 // exchange plan of one rank of a case split over ranks by block (mbm_create_sharded)
@@ -896,6 +901,7 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   for (int l = 0; l < 3; l++) cudaFree(c->buf[l]);
   cudaFree(c->rlx);
   cudaFree(c->dtmap);
+  cudaFree(c->dtma_drop);
   cudaFree(c->staging);
   cudaFree(c->dblk);
   cudaFree(c->dghost);

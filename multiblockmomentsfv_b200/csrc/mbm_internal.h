@@ -82,9 +82,10 @@ struct StageArgs {
   // plane); not null: the window slots are filled by bulk tensor copies (TMA) instead
   // of per-lane cp.async
   const void* tmap;
-  // failure-detection test only: 1 = warp 0 of CTA 0 withholds its first bulk copy, so
-  // that its bounded wait runs out (the host sets it for one launch)
-  int tma_drop;
+  // failure-detection test only (null otherwise): a device flag; while it is 1, warp 0 of
+  // CTA 0 consumes it (sets it to 0) and withholds its first bulk copy, so that its
+  // bounded wait runs out -- one launch, also when the launch is replayed from a graph
+  int* tma_drop;
 };
 
 constexpr int TMAP_BYTES = 128;   // sizeof(CUtensorMap)

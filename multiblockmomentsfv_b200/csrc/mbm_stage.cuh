@@ -591,7 +591,11 @@ __global__ void STAGE_BOUNDS stage_kernel(const StageArgs a) {
     // bulk tensor copies need 128-byte aligned slots (the window layout keeps them so
     // from an aligned base; otherwise the per-lane copies serve)
     tma = a.tmap != nullptr && (smem_u32(&win[warp]) & 127u) == 0;
-    drop = tma && a.tma_drop && blockIdx.x == 0 && warp == 0;
+    if (tma && a.tma_drop && blockIdx.x == 0 && warp == 0) {
+      int d = 0;
+      if (lane == 0) d = atomicExch(a.tma_drop, 0);
+      drop = __shfl_sync(0xffffffffu, d, 0) != 0;
+    }
     if (tma) {
       if (lane == 0) {
         mbar_init(&win[warp].bar[0]);
