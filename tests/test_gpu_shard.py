@@ -67,6 +67,41 @@ def test_split_equals_unsplit(case, mode):
         H.assert_bitwise(got[b], ref[b], f"block {b + 1}")
 
 
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+@pytest.mark.parametrize("max_steps,batch", [(5, 8), (13, 4), (7, 1)])
+def test_split_step_cap_within_a_batch(mode, max_steps, batch):
+    """The split loop enqueues `batch` attempts per host wait; a step cap that falls inside
+    a batch leaves the attempts after it as no-ops on the device: the same state, step
+    count and time as the unsplit solver capped at the same step, and two calls in a row
+    continue where the first stopped."""
+    import torch
+    d, scn = H.quadrant_deck(40, Kn=0.01, limiter=3), sc.Scenario.seeded_quadrant(6)
+    owner = [0, 1, 1, 0]
+    with sv.Solver(d, scn, mode=mode, show_every=0) as s:
+        s.initialise()
+        r1 = s.steps(0.0, 0.1, max_steps=max_steps)
+        r2 = s.steps(r1[0], 0.1, max_steps=max_steps)
+        ref = [s.download(sv.L_DATA, b) for b in range(len(d.blocks))]
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        parts = [sharded.ShardPart(d, owner, 2, r, scn, stream=stream.cuda_stream, mode=mode) for r in range(2)]
+        try:
+            ex = sharded.LocalExchange()
+            sharded.initialise(parts, scn, ex)
+            g1 = sharded.steps(parts, ex, 0.0, 0.1, max_steps=max_steps, batch=batch)
+            g2 = sharded.steps(parts, ex, g1[0], 0.1, max_steps=max_steps, batch=batch)
+            got = [None] * len(d.blocks)
+            for p in parts:
+                for g in p.blocks:
+                    got[g] = p.download(sv.L_DATA, g)
+        finally:
+            for p in parts:
+                p.close()
+    assert (g1, g2) == (r1, r2) and g1[1] == max_steps
+    for b in range(len(d.blocks)):
+        H.assert_bitwise(got[b], ref[b], f"block {b + 1}")
+
+
 def test_split_non_finite_stops_every_rank():
     import torch
     d, scn = H.quadrant_deck(48, Kn=0.01), sc.Scenario.seeded_quadrant(2)
