@@ -264,11 +264,16 @@ int mbm_shard_end(mbm_ctx *ctx, double *t, int *nsteps, int *nrej);
  * encoder always use the per-lane copies; the reason is then in mbm_last_error). */
 int mbm_bulk_copies(mbm_ctx *ctx, int *on);
 
-/* Launch configuration in use: rows per warp work item (picked by the autotuner
- * when mbm_params.segment_rows is 0; the tuner's length may be fractional -- a strip
- * of n face rows gets ceil(n / length) equal segments -- and is reported rounded),
- * work items per stage, CTAs of the persistent stage grid. */
+/* Launch configuration in use, of Heun stage 1: rows per warp work item (picked by
+ * the autotuner when mbm_params.segment_rows is 0; the tuner's length may be
+ * fractional -- a strip of n face rows gets ceil(n / length) equal segments -- and is
+ * reported rounded), work items, CTAs of the persistent stage grid. */
 int mbm_config(mbm_ctx *ctx, int *segment_rows, int *work_items, int *ctas);
+
+/* The same for either Heun stage (heun 0 or 1; each has its own work table, the
+ * tuner picking each stage's length), the length unrounded.  No counterpart in the
+ * reference. */
+int mbm_config_stage(mbm_ctx *ctx, int heun, double *segment_rows, int *work_items, int *ctas);
 
 /* Host-only: the resolved ghost-cell sources of a block table, 4 ints per ghost
  * cell {dst_block, dst_cell, src, src_block | flags<<16}; cells are J*(nx+6)+I,

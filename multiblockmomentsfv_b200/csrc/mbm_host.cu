@@ -100,12 +100,13 @@ struct mbm_ctx {
   std::vector<int> dir_off;         // [block*4+side] -> first Dirichlet row, -1 if none
   double* ddir = nullptr;
   int ndir = 0;
-  Work* dwork = nullptr;
-  int nwork = 0;
-  std::vector<LimGroup> groups;
+  Work* dwork = nullptr;            // the work tables of the two Heun stages, max_items apart
+  long long max_items = 0;
+  int nwork[2] = {0, 0};
+  std::vector<LimGroup> groups[2];  // limiter groups of each stage's table
   int nsm = 0, cta_warps = CTA_WARPS;   // stage kernel: warps per CTA
   int ctas_per_sm[2] = {1, 1};          // stage kernel: resident CTAs per SM of each Heun stage
-  double seg_rows = 0;              // rows per work item in use (ceil(rows / seg_rows) segments)
+  double seg_rows[2] = {0, 0};      // rows per work item of each Heun stage (ceil(rows / seg_rows) segments)
   CaseDev* dcase = nullptr;
   CaseDev* hcase = nullptr;         // pinned mirror, ncase entries
   unsigned long long* dlam = nullptr;
@@ -339,10 +340,11 @@ static int resolve_ghosts(const mbm_block_desc* B, int nb, std::vector<Resolved>
 static int pitch_of(int nxp) { return (nxp + 1 + 3) & ~3; }
 
 // Work items grouped by limiter (the stage kernel is specialised per limiter):
-// blocks of cases with limiter L fill group L, strips within row segments.
-static void build_work(mbm_ctx* c, double seg_rows, std::vector<Work>& w) {
+// blocks of cases with limiter L fill group L, strips within row segments.  Each Heun
+// stage has its own table (the autotuner picks each stage's segment length).
+static void build_work(mbm_ctx* c, double seg_rows, std::vector<Work>& w, std::vector<LimGroup>& groups) {
   w.clear();
-  c->groups.clear();
+  groups.clear();
   for (int lim = 0; lim < 5; lim++) {
     const int start = (int)w.size();
     for (int b = 0; b < c->nblk; b++) {
@@ -364,7 +366,7 @@ static void build_work(mbm_ctx* c, double seg_rows, std::vector<Work>& w) {
       for (int h = 0; h < 2; h++)
         g.grid[h] = (int)std::min<long long>((count + c->cta_warps - 1) / c->cta_warps,
                                              (long long)c->nsm * c->ctas_per_sm[h]);
-      c->groups.push_back(g);
+      groups.push_back(g);
     }
   }
 }
@@ -381,13 +383,18 @@ static long long count_items(const mbm_ctx* c, double seg_rows) {
   return n;
 }
 
-static int set_segments(mbm_ctx* c, double seg) {
-  std::vector<Work> work;
-  build_work(c, seg, work);
-  c->nwork = (int)work.size();
-  CK(cudaMemcpyAsync(c->dwork, work.data(), sizeof(Work) * work.size(), cudaMemcpyHostToDevice, c->stream));
+// the work table of stage h (0, 1; -1: both) for segments of `seg` rows
+static int set_segments(mbm_ctx* c, double seg, int h = -1) {
+  for (int k = 0; k < 2; k++) {
+    if (h >= 0 && k != h) continue;
+    std::vector<Work> work;
+    build_work(c, seg, work, c->groups[k]);
+    c->nwork[k] = (int)work.size();
+    CK(cudaMemcpyAsync(c->dwork + k * c->max_items, work.data(), sizeof(Work) * work.size(), cudaMemcpyHostToDevice,
+                       c->stream));
+    c->seg_rows[k] = seg;
+  }
   CK(cudaStreamSynchronize(c->stream));
-  c->seg_rows = seg;
   return MBM_OK;
 }
 
@@ -399,7 +406,8 @@ static int set_segments(mbm_ctx* c, double seg) {
 // ran on the same Data0 just before.
 static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, int sel_out, int rlx_read,
                                  double* const* bufs = nullptr) {
-  const int ng = (int)c->groups.size();
+  const std::vector<LimGroup>& groups = c->groups[heun];
+  const int ng = (int)groups.size();
   cudaError_t e0;
   if (ng > 1) {
     if ((e0 = cudaEventRecord(c->fork_ev, c->stream))) return e0;
@@ -407,11 +415,11 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
       if ((e0 = cudaStreamWaitEvent(c->aux[k - 1], c->fork_ev, 0))) return e0;
   }
   for (int k = 0; k < ng; k++) {
-    const LimGroup& g = c->groups[k];
+    const LimGroup& g = groups[k];
     cudaStream_t st = k == 0 ? c->stream : c->aux[k - 1];
     StageArgs a{};
     a.blk = c->dblk;
-    a.work = c->dwork + g.start;
+    a.work = c->dwork + heun * c->max_items + g.start;
     a.nwork = g.count;
     a.cases = c->dcase;
     for (int l = 0; l < 3; l++) a.buf[l] = bufs ? bufs[l] : c->buf[l];
@@ -460,23 +468,30 @@ static int push_cases(mbm_ctx* c) {
 // Autotuner: the stage kernel's work-item length (rows per warp segment) trades
 // the per-segment warm-up (two extra primitive rows, one slope row, one face row)
 // against load balance over the persistent grid.  On first use of a problem shape
-// it times both Heun stages for each candidate on a uniform state at rest and keeps
-// the fastest; the choice is cached per (strip rows, blocks, limiter mix, CTAs/SM)
-// for the life of the process.
+// it times each Heun stage for each candidate on a uniform state at rest and keeps,
+// per stage, the fastest (the two stages have their own work tables: at 4 x 1024^2
+// stage 1 ran best at 24 rows, stage 2 at 29); the choice is cached per (strip rows,
+// blocks, limiter mix, CTAs/SM) for the life of the process.
 static std::mutex g_tune_mu;
-static std::map<std::tuple<long long, int, int, int>, double> g_tune_cache;
+static std::map<std::tuple<long long, int, int, int>, std::array<double, 2>> g_tune_cache;
 
-static int time_both_stages(mbm_ctx* c, cudaEvent_t e0, cudaEvent_t e1, float* ms) {
-  for (int rep = 0; rep < 3; rep++) {
-    if (rep == 1) CK(cudaEventRecord(e0, c->stream));
-    for (int heun = 0; heun < 2; heun++) {
+// device time of each Heun stage with the current tables: one untimed pass of both,
+// then two timed launches of each stage
+static int time_each_stage(mbm_ctx* c, cudaEvent_t e0, cudaEvent_t e1, float* ms) {
+  for (int heun = 0; heun < 2; heun++) {
+    CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
+    CK(launch_stages(c, heun, heun ? SEL_TMP : SEL_CUR, SEL_CUR, heun ? SEL_OTHER : SEL_TMP, 1));
+  }
+  for (int heun = 0; heun < 2; heun++) {
+    CK(cudaEventRecord(e0, c->stream));
+    for (int rep = 0; rep < 2; rep++) {
       CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
       CK(launch_stages(c, heun, heun ? SEL_TMP : SEL_CUR, SEL_CUR, heun ? SEL_OTHER : SEL_TMP, 1));
     }
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(&ms[heun], e0, e1));
   }
-  CK(cudaEventRecord(e1, c->stream));
-  CK(cudaEventSynchronize(e1));
-  CK(cudaEventElapsedTime(ms, e0, e1));
   return MBM_OK;
 }
 
@@ -487,13 +502,16 @@ static int autotune(mbm_ctx* c) {
     cells += (long long)d.nxp * d.nyp;
   }
   int limmix = 0;
-  for (const LimGroup& g : c->groups) limmix |= 1 << g.lim;
+  for (const LimGroup& g : c->groups[0]) limmix |= 1 << g.lim;
   const auto key = std::make_tuple(strip_rows, c->nblk, limmix,
                                    (c->ctas_per_sm[0] * 256 + c->ctas_per_sm[1]) * c->cta_warps);
   {
     std::lock_guard<std::mutex> g(g_tune_mu);
     auto it = g_tune_cache.find(key);
-    if (it != g_tune_cache.end()) return set_segments(c, it->second);
+    if (it != g_tune_cache.end()) {
+      const int st = set_segments(c, it->second[0], 0);
+      return st ? st : set_segments(c, it->second[1], 1);
+    }
   }
   const char* env = getenv("MBM_AUTOTUNE");
   if (env && atoi(env) == 0) return set_segments(c, 32);
@@ -508,8 +526,8 @@ static int autotune(mbm_ctx* c) {
   LocalEvents ev;
   CK(cudaEventCreate(&ev.e[0]));
   CK(cudaEventCreate(&ev.e[1]));
-  double best = 32;
-  float best_ms = 1e30f;
+  double best[2] = {32, 32};
+  float best_ms[2] = {1e30f, 1e30f};
   // short segments buy parallelism on small grids, long ones save warm-up rows.  The
   // persistent grid's warps take the items from a queue, so the time jumps with the item
   // count: besides every even length, each wave count k gets the shortest length whose
@@ -533,12 +551,13 @@ static int autotune(mbm_ctx* c) {
       cand.push_back(hi);
     }
   }
-  for (double seg : cand) {
+  for (double seg : cand) {             // each stage keeps its own fastest length
     st = set_segments(c, seg);
-    float ms = 0.f;
-    if (!st) st = time_both_stages(c, ev.e[0], ev.e[1], &ms);
+    float ms[2] = {0.f, 0.f};
+    if (!st) st = time_each_stage(c, ev.e[0], ev.e[1], ms);
     if (st) return st;
-    if (ms < best_ms) { best_ms = ms; best = seg; }
+    for (int k = 0; k < 2; k++)
+      if (ms[k] < best_ms[k]) { best_ms[k] = ms[k]; best[k] = seg; }
   }
   for (int l = 0; l < 3; l++) CK(cudaMemsetAsync(c->buf[l], 0, sizeof(double) * c->layer_elems, c->stream));
   CK(cudaMemsetAsync(c->dlam, 0, sizeof(unsigned long long) * 6 * c->nblk, c->stream));
@@ -546,9 +565,10 @@ static int autotune(mbm_ctx* c) {
   if ((st = push_cases(c))) return st;
   {
     std::lock_guard<std::mutex> g(g_tune_mu);
-    g_tune_cache[key] = best;
+    g_tune_cache[key] = {best[0], best[1]};
   }
-  return set_segments(c, best);
+  st = set_segments(c, best[0], 0);
+  return st ? st : set_segments(c, best[1], 1);
 }
 
 // Tensor maps of the fast stage 2's bulk copies: for every block, its TMP layer and its
@@ -818,7 +838,8 @@ static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vecto
   c->cta_warps = c->fast ? fastmath::stage_cta_warps() : bitwise::stage_cta_warps();
   long long max_items = 0;
   for (auto& d : c->hblk) max_items += (long long)((d.nxp - 3 + STRIP - 1) / STRIP) * ((d.nyp - 3 + 7) / 8 + 1);
-  CKC(cudaMalloc(&c->dwork, sizeof(Work) * std::max<long long>(1, max_items)));
+  c->max_items = std::max<long long>(1, max_items);
+  CKC(cudaMalloc(&c->dwork, sizeof(Work) * 2 * c->max_items));
   {
     int st0 = params->segment_rows > 0 ? set_segments(c, std::max(8, params->segment_rows)) : autotune(c);
     if (st0) return bail(st0);
@@ -1219,9 +1240,9 @@ extern "C" int mbm_steps(mbm_ctx* c, double* t, double tend, double CFLmax, doub
 extern "C" int mbm_config(mbm_ctx* c, int* segment_rows, int* work_items, int* ctas) {
   if (!c) return fail(c, MBM_EINVAL, "mbm_config: null context");
   int g = 0;
-  for (const LimGroup& x : c->groups) g = std::max(g, std::max(x.grid[0], x.grid[1]));
-  if (segment_rows) *segment_rows = (int)std::lround(c->seg_rows);
-  if (work_items) *work_items = c->nwork;
+  for (const LimGroup& x : c->groups[0]) g = std::max(g, std::max(x.grid[0], x.grid[1]));
+  if (segment_rows) *segment_rows = (int)std::lround(c->seg_rows[0]);
+  if (work_items) *work_items = c->nwork[0];
   if (ctas) *ctas = g;
   return MBM_OK;
 }
@@ -1230,6 +1251,16 @@ extern "C" int mbm_bulk_copies(mbm_ctx* c, int* on) {
   if (!c || !on) return fail(c, MBM_EINVAL, "mbm_bulk_copies: bad argument");
   *on = c->dtmap != nullptr;
   if (!c->dtmap && !c->tma_note.empty()) c->err = c->tma_note;
+  return MBM_OK;
+}
+
+extern "C" int mbm_config_stage(mbm_ctx* c, int heun, double* segment_rows, int* work_items, int* ctas) {
+  if (!c || (heun != 0 && heun != 1)) return fail(c, MBM_EINVAL, "mbm_config_stage: bad argument");
+  int g = 0;
+  for (const LimGroup& x : c->groups[heun]) g = std::max(g, x.grid[heun]);
+  if (segment_rows) *segment_rows = c->seg_rows[heun];
+  if (work_items) *work_items = c->nwork[heun];
+  if (ctas) *ctas = g;
   return MBM_OK;
 }
 

@@ -180,10 +180,16 @@ class Solver:
         return a.value
 
     def config(self) -> dict:
-        """Launch configuration: rows per work item, work items, persistent CTAs."""
+        """Launch configuration: rows per work item, work items, persistent CTAs (stage 1),
+        and both stages' under "stages"."""
         a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
         self._check(self.L.mbm_config(self.ctx, C.byref(a), C.byref(b), C.byref(c)))
-        return {"segment_rows": a.value, "work_items": b.value, "ctas": c.value}
+        stages = []
+        for heun in (0, 1):
+            r, n, g = C.c_double(0.0), C.c_int(0), C.c_int(0)
+            self._check(self.L.mbm_config_stage(self.ctx, heun, C.byref(r), C.byref(n), C.byref(g)))
+            stages.append({"segment_rows": round(r.value, 3), "work_items": n.value, "ctas": g.value})
+        return {"segment_rows": a.value, "work_items": b.value, "ctas": c.value, "stages": stages}
 
     def bulk_copies(self) -> bool:
         """Whether the fast stage 2 fills its rows by bulk tensor copies (TMA)."""
