@@ -90,7 +90,7 @@ struct mbm_ctx {
   BlockDev* dblk = nullptr;
   long long layer_elems = 0;
   double* buf[3] = {nullptr, nullptr, nullptr};
-  double* rlx = nullptr;            // fast arithmetic: the stage-1 relaxation term (a layer)
+  double* rlx = nullptr;            // the relaxation term of Data0 stage 1 stores for stage 2 (a layer)
   void* dtmap = nullptr;            // fast arithmetic: per block, tensor maps of TMP and rlx (stage-2 TMA)
   std::string tma_note;             // why the stage-2 bulk tensor copies are off, if they are
   int* dtma_drop = nullptr;         // failure-detection test: device flag, the next bulk-copy launch withholds one copy
@@ -400,10 +400,10 @@ static int set_segments(mbm_ctx* c, double seg, int h = -1) {
 
 // one Heun stage of every block: one persistent launch per limiter group
 // (with several limiter groups, group k > 0 runs on aux stream k-1, so that one
-// group's CTAs fill the SMs another group's tail leaves idle).  rlx_read (stage 2,
-// fast arithmetic): the relaxation term of Data0 is read from what the stage 1 of
-// the same attempt stored, instead of being formed again -- only where that stage 1
-// ran on the same Data0 just before.
+// group's CTAs fill the SMs another group's tail leaves idle).  rlx_read (stage 2):
+// the relaxation term of Data0 is read from what the stage 1 of the same attempt
+// stored, instead of being formed again -- only where that stage 1 ran on the same
+// Data0 just before.
 static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, int sel_out, int rlx_read,
                                  double* const* bufs = nullptr) {
   const std::vector<LimGroup>& groups = c->groups[heun];
@@ -768,10 +768,8 @@ static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vecto
     CKC(cudaMalloc(&c->buf[l], sizeof(double) * off));
     CKC(cudaMemsetAsync(c->buf[l], 0, sizeof(double) * off, c->stream));
   }
-  if (c->fast) {
-    CKC(cudaMalloc(&c->rlx, sizeof(double) * off));
-    CKC(cudaMemsetAsync(c->rlx, 0, sizeof(double) * off, c->stream));
-  }
+  CKC(cudaMalloc(&c->rlx, sizeof(double) * off));
+  CKC(cudaMemsetAsync(c->rlx, 0, sizeof(double) * off, c->stream));
   CKC(cudaMalloc(&c->staging, sizeof(double) * max_cells * (NV + 1)));   // layers, or 10 output fields
   CKC(cudaMalloc(&c->dblk, sizeof(BlockDev) * nblocks));
   CKC(cudaMemcpyAsync(c->dblk, c->hblk.data(), sizeof(BlockDev) * nblocks, cudaMemcpyHostToDevice, c->stream));

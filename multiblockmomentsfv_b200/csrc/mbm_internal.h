@@ -71,10 +71,11 @@ struct StageArgs {
   int* queue;                // work-item counter of this stage (zero before the launch)
   int sel_in, sel_d0, sel_out;
   int heun;
-  // fast arithmetic only: the relaxation term of the stage-1 input (layer layout,
-  // interior cells), written by stage 1; rlx_read = 1 makes stage 2 read it in place
-  // of forming it again from Data0 (set only when the stage 1 of the same attempt,
-  // on the same Data0, ran just before)
+  // the relaxation term (flag -1) of the stage-1 input (layer layout, interior cells),
+  // written by stage 1 (fast arithmetic: never null, stage 1 reads it back; bitwise:
+  // null leaves it unwritten); rlx_read = 1 makes stage 2 read it in place of forming
+  // it again from Data0 (set only when the stage 1 of the same attempt, on the same
+  // Data0, ran just before)
   double* rlx;
   int rlx_read;
   // fast arithmetic, stage 2 with rlx_read: 2 tensor maps (CUtensorMap, 128 bytes each)

@@ -285,21 +285,27 @@ __device__ __forceinline__ double rdamp(double z) {
   return fdiv(1.0, 1 + 0.5 * z);
 }
 
-// ProductionsDirect (src/Flux.c:230-267) with CollFreq and ExternalForce
-// (src/Scenario.c:28-42; nu0 = 1, force (F, 0)), starting from the primitives P
-// of the input moments.  Writes the relaxed moments, returns 0.5*(1 - R(2z/3)).
+// The collision number z = dt nu0 rho sqrt(theta) / Kn of ProductionsDirect
+// (src/Flux.c:230-267 with CollFreq, src/Scenario.c:28-42; nu0 = 1): the same
+// expression for every flag, so one evaluation serves all of a cell's flags.  Kn is in
+// the safe range (checked when the kernel starts); the numerator's range decides
+// between the shared-reciprocal quotient and IEEE division.
+__device__ __forceinline__ double coll_of(const double (&P)[NV], double dt, const Recip& Kn) {
+  const double nu0 = 1.0;
+  const double num = nu0 * P[0] * fsqrt(P[3]);
+  return (__builtin_expect(mk_in(num), 1) ? Kn.exact(num) : div_ieee(num, Kn.y)) * dt;
+}
+
+// ProductionsDirect (src/Flux.c:230-267) with ExternalForce (src/Scenario.c:28-42;
+// force (F, 0)), starting from the primitives P of the input moments, given its damping
+// factors d1 = rdamp<FLAG>(z), d2 = rdamp<FLAG>(2z/3).  Writes the relaxed moments.
 template <int FLAG>
-__device__ __forceinline__ double relax(const double (&P)[NV], double (&Out)[NV], double dt,
-                                        const Recip& Kn, double F) {
-  // Kn is in the safe range (checked when the kernel starts); the numerator's range
-  // decides between the shared-reciprocal quotient and IEEE division
+__device__ __forceinline__ void relax_d(const double (&P)[NV], double (&Out)[NV], double dt, double F,
+                                        double d1, double d2) {
   const double rho = P[0], th = P[3];
   double v1 = P[1], v2 = P[2];
   double vs = v1 * v1 + v2 * v2;
   double E = 0.5 * rho * vs + 1.5 * rho * th;
-  const double nu0 = 1.0;
-  const double num = nu0 * rho * fsqrt(th);
-  const double coll = (__builtin_expect(mk_in(num), 1) ? Kn.exact(num) : div_ieee(num, Kn.y)) * dt;
   if (FLAG == 0 || FLAG == 2) {
     const double g0 = F, g1 = 0.0;
     v1 += dt * g0;
@@ -307,12 +313,21 @@ __device__ __forceinline__ double relax(const double (&P)[NV], double (&Out)[NV]
     vs = v1 * v1 + v2 * v2;
     E = 0.5 * rho * vs + 1.5 * rho * th;
   }
-  const double d1 = rdamp<FLAG>(coll);
-  const double d2 = rdamp<FLAG>(2.0 / 3 * coll);
   const double T11 = d1 * (P[4] - th) + th;
   const double T12 = d1 * P[5];
   const double T22 = d1 * (P[6] - th) + th;
   moments_e(rho, v1, v2, E, T11, T12, T22, d2 * P[7], d2 * P[8], Out);
+}
+
+// ProductionsDirect of flag FLAG from the primitives P: writes the relaxed moments,
+// returns 0.5*(1 - R(2z/3))
+template <int FLAG>
+__device__ __forceinline__ double relax(const double (&P)[NV], double (&Out)[NV], double dt,
+                                        const Recip& Kn, double F) {
+  const double coll = coll_of(P, dt, Kn);
+  const double d1 = rdamp<FLAG>(coll);
+  const double d2 = rdamp<FLAG>(2.0 / 3 * coll);
+  relax_d<FLAG>(P, Out, dt, F, d1, d2);
   return 0.5 * (1 - d2);
 }
 
@@ -393,10 +408,7 @@ __device__ __forceinline__ void push_moments(const double (&U)[NV], double g, do
 // only the CFL share of relax<FLAG> (same z, same factor)
 template <int FLAG>
 __device__ __forceinline__ double relax_cfl(const double (&P)[NV], double dt, const Recip& Kn) {
-  const double nu0 = 1.0;
-  const double num = nu0 * P[0] * fsqrt(P[3]);
-  const double coll = (__builtin_expect(mk_in(num), 1) ? Kn.exact(num) : div_ieee(num, Kn.y)) * dt;
-  return 0.5 * (1 - rdamp<FLAG>(2.0 / 3 * coll));
+  return 0.5 * (1 - rdamp<FLAG>(2.0 / 3 * coll_of(P, dt, Kn)));
 }
 
 // Limit1 (src/Limiter.c:26-59)

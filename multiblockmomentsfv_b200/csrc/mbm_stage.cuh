@@ -154,16 +154,13 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
   const double* __restrict__ in = a.buf[phys_layer(a.sel_in, cur)] + B.off;
   const double* __restrict__ d0 = a.buf[phys_layer(a.sel_d0, cur)] + B.off;
   double* __restrict__ out = a.buf[phys_layer(a.sel_out, cur)] + B.off;
-#if MBM_FAST_ARITH
-  // the relaxation term of the stage-1 input: written by stage 1 at its row r and read
-  // back (plain loads: written in this launch) by the update of that row two
-  // iterations later; stage 2 reads it with rlx_read in place of forming it from Data0
-  double* __restrict__ rlx = a.rlx + B.off;
+  // the relaxation term of the stage-1 input (flag -1): written by stage 1 at its row r
+  // (fast arithmetic: read back, with plain loads, by the update of that row two
+  // iterations later); stage 2 reads it with rlx_read in place of forming it from
+  // Data0.  Null (bitwise only): not stored.
+  double* __restrict__ rlx = a.rlx ? a.rlx + B.off : nullptr;
   const bool rlx_rd = HEUN == 1 && a.rlx_read;
   const double* __restrict__ d0src = rlx_rd ? rlx : d0;
-#else
-  const double* __restrict__ d0src = d0;
-#endif
   const int nxp = B.nxp, nyp = B.nyp, pitch = B.pitch;
   const long long plane = B.plane;
   const int C = w.I0 - 2 + lane;
@@ -322,10 +319,33 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
         }
       }
 #endif
-      if (!MBM_FAST_ARITH && ok && col_cell && r >= 1 && r <= nyp - 2) {
-        const double c = relax_cfl<2 * HEUN>(Q, dt, Kn);
+#if !MBM_FAST_ARITH
+      // one collision number serves every ProductionsDirect of this cell in this stage,
+      // each flag's damping factors formed from it with the reference's expressions:
+      // the CFL share and the update's relaxation term (flag 2 HEUN, parked in the
+      // output layer until the update of this row two iterations later), stage 1's
+      // relaxation of Data0 for stage 2 (flag -1: flag 0 without the force) and the
+      // projection (flag 2 HEUN + 1)
+      const double z = coll_of(Q, dt, Kn);
+      const double d2u = rdamp<2 * HEUN>(2.0 / 3 * z);
+      if (ok && col_cell && r >= 1 && r <= nyp - 2) {
+        const double c = 0.5 * (1 - d2u);
         if (c > prod) prod = c;
       }
+      if (ok && col_out && r >= NG && r <= nyp - 1 - NG && r >= w.J0 && r < w.J1) {
+        const double d1u = rdamp<2 * HEUN>(z);
+        const long long idx = (long long)r * pitch + C + 1;
+        double R[NV];
+        relax_d<2 * HEUN>(Q, R, dt, Fx, d1u, d2u);
+#pragma unroll
+        for (int n = 0; n < NV; n++) out[n * plane + idx] = R[n];
+        if (HEUN == 0 && rlx) {
+          relax_d<-1>(Q, R, dt, Fx, d1u, d2u);
+#pragma unroll
+          for (int n = 0; n < NV; n++) rlx[n * plane + idx] = R[n];
+        }
+      }
+#endif
       if (!(col_ring || r == 0 || r == nyp - 1)) {
 #if MBM_FAST_ARITH
         if (HEUN == 1) {   // stage 2 (flag 3): no CFL share (flag 2 is the identity)
@@ -336,7 +356,7 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
         }
 #else
         double V[NV];
-        relax<2 * HEUN + 1>(Q, V, dt, Kn, Fx);
+        relax_d<2 * HEUN + 1>(Q, V, dt, Fx, rdamp<2 * HEUN + 1>(z), rdamp<2 * HEUN + 1>(2.0 / 3 * z));
         primitive(V, Q);
 #endif
       }
@@ -479,15 +499,14 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
           for (int n = 0; n < NV; n++) R[n] = U[n];
         }
 #else
-        load_cell(in, plane, idx, U);
-        primitive(U, Q);
-        relax<2 * HEUN>(Q, R, dt, Kn, Fx);
+        // relax<2 HEUN> of this cell, parked here by the window pass (plain loads)
+#pragma unroll
+        for (int n = 0; n < NV; n++) R[n] = out[n * plane + idx];
 #endif
         if constexpr (HEUN == 1) {
           double R0[NV];
 #pragma unroll
           for (int n = 0; n < NV; n++) U[n] = win.D0a[n][lane];
-#if MBM_FAST_ARITH
           if (rlx_rd) {                       // relax<-1>(Data0), stored by stage 1
 #pragma unroll
             for (int n = 0; n < NV; n++) R0[n] = U[n];
@@ -495,10 +514,6 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
             primitive(U, Q);
             relax<-1>(Q, R0, dt, Kn, Fx);
           }
-#else
-          primitive(U, Q);
-          relax<-1>(Q, R0, dt, Kn, Fx);
-#endif
 #pragma unroll
           for (int n = 0; n < NV; n++) R[n] += R0[n];
         }
