@@ -428,6 +428,7 @@ def main():
     attempts = s.attempts()
     launch = s.config()
     launch["stage2_bulk_tensor_copies"] = s.bulk_copies()
+    launch["ghost_fill_in_stage_kernels"] = s.ghost_scatter()
     ms = e0.elapsed_time(e1)
     barrier()
     ms_max = ms

@@ -275,6 +275,14 @@ int mbm_config(mbm_ctx *ctx, int *segment_rows, int *work_items, int *ctas);
  * reference. */
 int mbm_config_stage(mbm_ctx *ctx, int heun, double *segment_rows, int *work_items, int *ctas);
 
+/* *on = 1 when the step loop's ghost fills (SetBoundary after each stage,
+ * src/Boundary.c:173-193) are done inside the stage kernels, each work item writing the
+ * ghost cells whose source cells it stored (for a Dirichlet ghost: whose nearest
+ * interior cell it stored) -- opt-in, MBM_GHOST_SCATTER=1 at context creation; 0 when a
+ * separate gather launch fills them (the default; always in sharded contexts).  Both
+ * give the same layers bit for bit. */
+int mbm_ghost_scatter(mbm_ctx *ctx, int *on);
+
 /* Host-only: the resolved ghost-cell sources of a block table, 4 ints per ghost
  * cell {dst_block, dst_cell, src, src_block | flags<<16}; cells are J*(nx+6)+I,
  * src < 0 is Dirichlet row -(src+1), flags bit 0/1 = x/y wall sign.  Needs no GPU. */

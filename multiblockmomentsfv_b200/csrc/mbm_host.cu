@@ -100,6 +100,15 @@ struct mbm_ctx {
   std::vector<int> dir_off;         // [block*4+side] -> first Dirichlet row, -1 if none
   double* ddir = nullptr;
   int ndir = 0;
+  // SetBoundary fused into the stage kernel: the ghost fill of each stage's output
+  // scattered by the work items that write its sources (opt-in, MBM_GHOST_SCATTER=1:
+  // at 4 x 1024^2 the separate gather launch costs less; never in a sharded context,
+  // whose remote ghosts arrive from other ranks)
+  bool gscatter = false;
+  std::vector<int> gs_cell;          // host: per cell of every block (off / 9 + element), its first owned entry
+  std::vector<GhostScatter> gs_ent;  // host: the entries in owner order
+  GhostScatter* dgs = nullptr;       // per stage (gs_ent.size() apart): the entries in work-item order
+  int2* dgs_item = nullptr;          // per stage (max_items apart): first entry and count of each item
   Work* dwork = nullptr;            // the work tables of the two Heun stages, max_items apart
   long long max_items = 0;
   int nwork[2] = {0, 0};
@@ -383,6 +392,46 @@ static long long count_items(const mbm_ctx* c, double seg_rows) {
   return n;
 }
 
+// The ghost-fill entries of the work items of stage k's table: each item lists the
+// entries owned by the cells it writes (output columns [I0, I0+28) and rows [J0, J1)
+// within the interior; owners lie within NG of an edge).  Every entry belongs to
+// exactly one item; if not, the separate gather fills the ghosts instead.
+static int set_item_scatter(mbm_ctx* c, int k, const std::vector<Work>& work) {
+  if (!c->gscatter) return MBM_OK;
+  std::vector<int2> items(work.size());
+  std::vector<GhostScatter> ents;
+  ents.reserve(c->gs_ent.size());
+  for (size_t i = 0; i < work.size(); i++) {
+    const Work& w = work[i];
+    const BlockDev& B = c->hblk[w.blk];
+    const long long cb = B.off / NV;
+    const int c0 = std::max(w.I0, NG), c1 = std::min(w.I0 + STRIP, B.nxp - NG);
+    const int j0 = std::max(w.J0, NG), j1 = std::min(w.J1, B.nyp - NG);
+    const int first = (int)ents.size();
+    for (int J = j0; J < j1; J++) {
+      const bool band_row = J < 2 * NG || J >= B.nyp - 2 * NG;
+      for (int C = c0; C < c1; C++) {
+        if (!band_row && C >= 2 * NG && C < B.nxp - 2 * NG) {
+          C = B.nxp - 2 * NG - 1;      // on to the right band
+          continue;
+        }
+        const size_t q = (size_t)(cb + (long long)J * B.pitch + C + 1);
+        for (int e = c->gs_cell[q]; e < c->gs_cell[q + 1]; e++) ents.push_back(c->gs_ent[e]);
+      }
+    }
+    items[i] = make_int2(first, (int)ents.size() - first);
+  }
+  if (ents.size() != c->gs_ent.size()) {
+    c->gscatter = false;
+    return MBM_OK;
+  }
+  CK(cudaMemcpyAsync(c->dgs + (size_t)k * c->gs_ent.size(), ents.data(), sizeof(GhostScatter) * ents.size(),
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->dgs_item + (size_t)k * c->max_items, items.data(), sizeof(int2) * items.size(),
+                     cudaMemcpyHostToDevice, c->stream));
+  return MBM_OK;
+}
+
 // the work table of stage h (0, 1; -1: both) for segments of `seg` rows
 static int set_segments(mbm_ctx* c, double seg, int h = -1) {
   for (int k = 0; k < 2; k++) {
@@ -392,6 +441,8 @@ static int set_segments(mbm_ctx* c, double seg, int h = -1) {
     c->nwork[k] = (int)work.size();
     CK(cudaMemcpyAsync(c->dwork + k * c->max_items, work.data(), sizeof(Work) * work.size(), cudaMemcpyHostToDevice,
                        c->stream));
+    const int st = set_item_scatter(c, k, work);
+    if (st) return st;
     c->seg_rows[k] = seg;
   }
   CK(cudaStreamSynchronize(c->stream));
@@ -405,7 +456,7 @@ static int set_segments(mbm_ctx* c, double seg, int h = -1) {
 // stored, instead of being formed again -- only where that stage 1 ran on the same
 // Data0 just before.
 static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, int sel_out, int rlx_read,
-                                 double* const* bufs = nullptr) {
+                                 double* const* bufs = nullptr, bool fill = false) {
   const std::vector<LimGroup>& groups = c->groups[heun];
   const int ng = (int)groups.size();
   cudaError_t e0;
@@ -433,6 +484,11 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
     // and rlx; the adjoint's recomputation passes other buffers and keeps cp.async)
     a.tmap = (c->fast && a.rlx_read && !bufs) ? c->dtmap : nullptr;
     if (a.tmap) a.tma_drop = c->dtma_drop;   // consumed on the device by the first launch
+    if (fill && c->gscatter) {                // the output layer's ghost fill, scattered
+      a.gs_item = c->dgs_item + heun * c->max_items + g.start;
+      a.gs = c->dgs + heun * c->gs_ent.size();
+      a.dirichlet = c->ddir;
+    }
     cudaError_t e = c->fast ? fastmath::launch_stage(g.lim, a, g.grid[heun], st)
                             : bitwise::launch_stage(g.lim, a, g.grid[heun], st);
     if (e != cudaSuccess) return e;
@@ -444,13 +500,15 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
   return cudaSuccess;
 }
 
-// the body of one step attempt: stage 1, fill TMP, stage 2, fill NEW, controller
+// the body of one step attempt: stage 1, fill TMP, stage 2, fill NEW, controller (the
+// fills inside the stage kernels when they scatter them)
 static cudaError_t launch_attempt(mbm_ctx* c, cudaGraphConditionalHandle h, int use_handle) {
   cudaError_t e;
-  if ((e = launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP, 0))) return e;
-  if ((e = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_TMP, c->stream))) return e;
-  if ((e = launch_stages(c, 1, SEL_TMP, SEL_CUR, SEL_OTHER, 1))) return e;
-  if ((e = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_OTHER, c->stream))) return e;
+  const bool g = !c->gscatter;
+  if ((e = launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP, 0, nullptr, true))) return e;
+  if (g && (e = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_TMP, c->stream))) return e;
+  if ((e = launch_stages(c, 1, SEL_TMP, SEL_CUR, SEL_OTHER, 1, nullptr, true))) return e;
+  if (g && (e = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_OTHER, c->stream))) return e;
   if ((e = launch_control(c->dcase, c->ncase, c->dblk, c->dlam, c->dtrace, c->dqueue, h, use_handle, c->stream)))
     return e;
   if (c->adjoint) return launch_ckpt(c->dcase, c->buf[0], c->buf[1], c->layer_elems, 4 * c->nsm, c->stream);
@@ -804,6 +862,54 @@ static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vecto
     CKC(cudaMemcpyAsync(c->dghost, gm.data(), sizeof(GhostEntry) * gm.size(), cudaMemcpyHostToDevice, c->stream));
   CKC(cudaMalloc(&c->ddir, sizeof(double) * NV * std::max(1, ndir)));
   CKC(cudaMemsetAsync(c->ddir, 0, sizeof(double) * NV * std::max(1, ndir), c->stream));
+  {
+    // the same fill listed under owners: a copied ghost under its source, a Dirichlet
+    // ghost under the interior cell nearest to it; every owner must be an interior cell
+    // within NG of its block's edge, else the gather stays
+    const char* env = getenv("MBM_GHOST_SCATTER");
+    bool ok = env && atoi(env) == 1 && !res.empty();
+    std::vector<std::pair<long long, GhostScatter>> lst;
+    lst.reserve(res.size());
+    for (size_t i = 0; ok && i < res.size(); i++) {
+      const Resolved& r = res[i];
+      if (r.remote >= 0) { ok = false; break; }
+      const BlockDev& D = c->hblk[r.dst_blk];
+      int ob = r.dst_blk, oI, oJ;
+      if (r.src >= 0) {
+        ob = r.src_blk;
+        oI = r.src % c->hblk[ob].nxp;
+        oJ = r.src / c->hblk[ob].nxp;
+      } else {
+        oI = std::min(std::max(r.dst_cell % D.nxp, NG), D.nxp - 1 - NG);
+        oJ = std::min(std::max(r.dst_cell / D.nxp, NG), D.nyp - 1 - NG);
+      }
+      const BlockDev& O = c->hblk[ob];
+      const bool interior = oI >= NG && oI <= O.nxp - 1 - NG && oJ >= NG && oJ <= O.nyp - 1 - NG;
+      const bool band = oI < 2 * NG || oI >= O.nxp - 2 * NG || oJ < 2 * NG || oJ >= O.nyp - 2 * NG;
+      if (!interior || !band) { ok = false; break; }
+      GhostScatter g;
+      g.dst = D.off + gm[i].dst;
+      g.plane = D.plane;
+      g.src = oJ * O.pitch + oI + 1;
+      g.flags = r.flags & 3;
+      g.drow = r.src >= 0 ? -1 : -(r.src + 1);
+      g.pad_ = 0;
+      lst.emplace_back(O.off / NV + g.src, g);
+    }
+    if (ok) {     // owner order (the tables of the work items are built from it)
+      std::stable_sort(lst.begin(), lst.end(),
+                       [](const std::pair<long long, GhostScatter>& x, const std::pair<long long, GhostScatter>& y) {
+                         return x.first < y.first;
+                       });
+      const long long ncell = c->layer_elems / NV;
+      c->gs_cell.assign((size_t)ncell + 1, 0);
+      for (auto& p : lst) c->gs_cell[(size_t)p.first + 1]++;
+      for (long long k = 0; k < ncell; k++) c->gs_cell[(size_t)k + 1] += c->gs_cell[(size_t)k];
+      c->gs_ent.resize(lst.size());
+      for (size_t i = 0; i < lst.size(); i++) c->gs_ent[i] = lst[i].second;
+      c->gscatter = true;
+    }
+  }
 
   // controllers, maxima, queues, trace, per-block CFL
   CKC(cudaMalloc(&c->dcase, sizeof(CaseDev) * ncases));
@@ -838,6 +944,10 @@ static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vecto
   for (auto& d : c->hblk) max_items += (long long)((d.nxp - 3 + STRIP - 1) / STRIP) * ((d.nyp - 3 + 7) / 8 + 1);
   c->max_items = std::max<long long>(1, max_items);
   CKC(cudaMalloc(&c->dwork, sizeof(Work) * 2 * c->max_items));
+  if (c->gscatter) {
+    CKC(cudaMalloc(&c->dgs, sizeof(GhostScatter) * 2 * c->gs_ent.size()));
+    CKC(cudaMalloc(&c->dgs_item, sizeof(int2) * 2 * c->max_items));
+  }
   {
     int st0 = params->segment_rows > 0 ? set_segments(c, std::max(8, params->segment_rows)) : autotune(c);
     if (st0) return bail(st0);
@@ -925,6 +1035,8 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   cudaFree(c->dblk);
   cudaFree(c->dghost);
   cudaFree(c->ddir);
+  cudaFree(c->dgs);
+  cudaFree(c->dgs_item);
   cudaFree(c->dwork);
   cudaFree(c->dcase);
   if (c->hcase) cudaFreeHost(c->hcase);
@@ -1252,6 +1364,12 @@ extern "C" int mbm_bulk_copies(mbm_ctx* c, int* on) {
   return MBM_OK;
 }
 
+extern "C" int mbm_ghost_scatter(mbm_ctx* c, int* on) {
+  if (!c || !on) return fail(c, MBM_EINVAL, "mbm_ghost_scatter: bad argument");
+  *on = c->gscatter ? 1 : 0;
+  return MBM_OK;
+}
+
 extern "C" int mbm_config_stage(mbm_ctx* c, int heun, double* segment_rows, int* work_items, int* ctas) {
   if (!c || (heun != 0 && heun != 1)) return fail(c, MBM_EINVAL, "mbm_config_stage: bad argument");
   int g = 0;
@@ -1412,11 +1530,11 @@ static int frozen_step(mbm_ctx* c, const double* in, double* out, const double* 
   double* bufs[3] = {const_cast<double*>(in), out, tmp};
   CK(cudaMemcpyAsync(&c->dcase[0].dt, ddt, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
-  CK(launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP, 0, bufs));
-  CK(launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, bufs, c->ddir, SEL_TMP, c->stream));
+  CK(launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP, 0, bufs, true));
+  if (!c->gscatter) CK(launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, bufs, c->ddir, SEL_TMP, c->stream));
   if (!out) return MBM_OK;
-  CK(launch_stages(c, 1, SEL_TMP, SEL_CUR, SEL_OTHER, 1, bufs));
-  CK(launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, bufs, c->ddir, SEL_OTHER, c->stream));
+  CK(launch_stages(c, 1, SEL_TMP, SEL_CUR, SEL_OTHER, 1, bufs, true));
+  if (!c->gscatter) CK(launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, bufs, c->ddir, SEL_OTHER, c->stream));
   return MBM_OK;
 }
 

@@ -46,6 +46,19 @@ struct GhostEntry {    // final value of one ghost cell after the two-sweep fill
   int src_blk_flags;   // src_blk | (x-wall flip << 16) | (y-wall flip << 17) | GHOST_REMOTE
 };
 
+// The ghost fill scattered from its sources (SetBoundary fused into the stage kernel):
+// one entry per ghost cell, listed under the work item that writes its owner -- the
+// interior cell it is copied from, or, for a Dirichlet ghost, the interior cell nearest
+// to it
+struct GhostScatter {
+  long long dst;       // element index of the ghost cell in the layer (block offset included)
+  long long plane;     // plane stride of the ghost cell's block
+  int src;             // element index of the owner in its block (the work item's block)
+  int flags;           // x-wall flip | y-wall flip << 1
+  int drow;            // >= 0: Dirichlet row (the value comes from the table); -1: a copy of the owner
+  int pad_;
+};
+
 struct CaseDev {       // per-case step controller (src/Main.c:189-244)
   double t, tend, dt, CFLmax, CFLreg, Kn, F;
   double cfl_last;
@@ -83,6 +96,12 @@ struct StageArgs {
   // plane); not null: the window slots are filled by bulk tensor copies (TMA) instead
   // of per-lane cp.async
   const void* tmap;
+  // the ghost fill of the output layer, done by the work items that write the owners
+  // (null: not done here; a separate gather fills the ghosts).  gs_item[w]: the first
+  // entry of gs and the entry count of work item w
+  const int2* gs_item;
+  const GhostScatter* gs;
+  const double* dirichlet;   // Dirichlet rows (9 values each)
   // failure-detection test only (null otherwise): a device flag; while it is 1, warp 0 of
   // CTA 0 consumes it (sets it to 0) and withholds its first bulk copy, so that its
   // bounded wait runs out -- one launch, also when the launch is replayed from a graph

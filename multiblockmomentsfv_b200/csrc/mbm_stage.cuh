@@ -138,10 +138,31 @@ constexpr int STAGE_WARPS = STAGE_CTA_WARPS;
 // slots by bulk tensor copies; tma: whether it does (warp-uniform; ph holds the phase
 // bits of the warp's two window barriers across items).  The instantiation without it
 // carries only the per-lane copies: the unused branches alone cost 4 % of stage 2.
+// SetBoundary (src/Boundary.c:173-193) fused into the stage: once a work item's cells
+// are stored, its warp writes the ghost cells whose owners the item wrote, one entry per
+// lane -- the owner's value read back from the output layer, or the Dirichlet row --
+// sign-flipped on the wall components as the gather does
+__device__ __forceinline__ void scatter_item(const StageArgs& a, int wi, int lane, double* base,
+                                             const double* out, long long plane) {
+  const int2 r = a.gs_item[wi];
+  if (r.y <= 0) return;
+  __syncwarp();     // every lane's stores of this item are visible to the warp
+  for (int e = r.x + lane; e < r.x + r.y; e += 32) {
+    const GhostScatter g = a.gs[e];
+    const bool fx = g.flags & 1, fy = (g.flags >> 1) & 1;
+#pragma unroll
+    for (int m = 0; m < NV; m++) {
+      const double v = g.drow < 0 ? out[m * plane + g.src] : __ldg(a.dirichlet + (size_t)g.drow * NV + m);
+      const bool flip = (fx && (m == 1 || m == 5 || m == 7)) != (fy && (m == 2 || m == 5 || m == 8));
+      base[g.dst + m * g.plane] = flip ? -v : v;
+    }
+  }
+}
+
 // Returns false when a bounded wait on a copy ran out: the case is flagged (the
 // controller stops it with a timeout status) and the warp stops taking items.
 template <int HEUN, int LIM, bool TMA>
-__device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, const int lane,
+__device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, const int wi, const int lane,
                                            WarpWindow<HEUN>& win, const bool tma_on, unsigned& ph,
                                            bool& drop) {
   const bool tma = TMA && tma_on;
@@ -558,6 +579,7 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
       cp_async_wait_all();
     }
   }
+  if (a.gs_item) scatter_item(a, wi, lane, out - B.off, out, plane);
 
   // per-block maxima; the values are >= 0 (or NaN, which never passes a '>' test
   // above), so their bit patterns order like the values
@@ -626,7 +648,7 @@ __global__ void STAGE_BOUNDS stage_kernel(const StageArgs a) {
     if (lane == 0) w = atomicAdd(a.queue, 1);
     w = __shfl_sync(0xffffffffu, w, 0);
     if (w >= a.nwork) break;
-    if (!stage_item<HEUN, LIM, TMA>(a, a.work[w], lane, win[warp], tma, ph, drop)) break;
+    if (!stage_item<HEUN, LIM, TMA>(a, a.work[w], w, lane, win[warp], tma, ph, drop)) break;
   }
 }
 

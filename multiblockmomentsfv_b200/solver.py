@@ -197,6 +197,12 @@ class Solver:
         self._check(self.L.mbm_bulk_copies(self.ctx, C.byref(on)))
         return bool(on.value)
 
+    def ghost_scatter(self) -> bool:
+        """Whether the step loop's ghost fills are done inside the stage kernels."""
+        on = C.c_int(0)
+        self._check(self.L.mbm_ghost_scatter(self.ctx, C.byref(on)))
+        return bool(on.value)
+
     def time_stage(self, heun: int, dt: float, reps: int = 10) -> float:
         """Mean device milliseconds of one stage-kernel launch (CUDA events)."""
         ms = C.c_double(0.0)
