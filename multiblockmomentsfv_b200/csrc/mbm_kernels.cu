@@ -28,8 +28,8 @@ __global__ void ghost_kernel(const BlockDev* __restrict__ blk, const CaseDev* __
   const BlockDev D = blk[e.dst_blk];
   const CaseDev& cs = cases[D.case_id];
   if (cs.done) return;
-  double* bufs[3] = {buf0, buf1, buf2};
-  double* layer = bufs[phys_layer(sel, cs.cur)];
+  const int l = phys_layer(sel, cs.cur);
+  double* layer = l == 0 ? buf0 : (l == 1 ? buf1 : buf2);
   double* dst = layer + D.off + e.dst;
   const int sblk = e.src_blk_flags & 0xffff;
   const bool fx = (e.src_blk_flags >> 16) & 1, fy = (e.src_blk_flags >> 17) & 1;
@@ -291,8 +291,8 @@ __global__ void shard_pack_kernel(const BlockDev* __restrict__ blk, const CaseDe
   const int i = (int)(t / NV), m = (int)(t - (long long)i * NV);
   const int2 e = list[i];
   const BlockDev B = blk[e.x];
-  const double* bufs[3] = {buf0, buf1, buf2};
-  const double* layer = bufs[phys_layer(sel, cases[0].cur)];
+  const int l = phys_layer(sel, cases[0].cur);
+  const double* layer = l == 0 ? buf0 : (l == 1 ? buf1 : buf2);
   send[t] = layer[B.off + m * B.plane + e.y];
 }
 

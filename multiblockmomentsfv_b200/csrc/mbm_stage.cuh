@@ -172,9 +172,9 @@ __device__ __forceinline__ bool stage_item(const StageArgs& a, const Work w, con
   const int cur = cs.cur;
   const double dt = cs.dt, Fx = cs.F;
   const Recip Kn(cs.Kn);
-  const double* __restrict__ in = a.buf[phys_layer(a.sel_in, cur)] + B.off;
-  const double* __restrict__ d0 = a.buf[phys_layer(a.sel_d0, cur)] + B.off;
-  double* __restrict__ out = a.buf[phys_layer(a.sel_out, cur)] + B.off;
+  const double* __restrict__ in = layer_ptr(a.buf, phys_layer(a.sel_in, cur)) + B.off;
+  const double* __restrict__ d0 = layer_ptr(a.buf, phys_layer(a.sel_d0, cur)) + B.off;
+  double* __restrict__ out = layer_ptr(a.buf, phys_layer(a.sel_out, cur)) + B.off;
   // the relaxation term of the stage-1 input (flag -1): written by stage 1 at its row r
   // (fast arithmetic: read back, with plain loads, by the update of that row two
   // iterations later); stage 2 reads it with rlx_read in place of forming it from
