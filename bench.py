@@ -241,6 +241,42 @@ def exact_leg(a, d, scn, local, stream):
                              / measured_peaks()[0]}
 
 
+def ffs_leg(a, local, stream, headline):
+    """Many small blocks: the forward-facing-step layout of the reference's cases/ffs28.txt
+    (28 blocks, a Dirichlet inflow edge, walls around the step, interfaces between all
+    blocks), each block refined by --ffs-refine; the same step loop and stage kernel, the
+    work table spread over 28 blocks -- its load balance against the 4-block headline.
+    The deck's own limiter (average: unlimited slopes) goes non-finite at the step's shock
+    once the blocks are refined 32 times (both arithmetic modes), so the leg runs the
+    headline's harmonic limiter."""
+    import torch
+    from multiblockmomentsfv_b200 import blockfile as bf, scenario as sc, solver as sv
+    d = bf.parse_file(os.path.join(ROOT, "tests", "golden", "decks", "ffs28.txt"), refine=a.ffs_refine)
+    d.limiter = bf.LIM_HARMONIC
+    scn = sc.Scenario.named("ffs")
+    cells = d.full_grid_size
+    with sv.Solver(d, scn, device=local, show_every=0, stream=stream.cuda_stream,
+                   segment_rows=a.segment_rows, mode=a.mode) as s:
+        s.initialise()
+        t, _, _ = s.steps(0.0, 10.0, max_steps=a.warmup)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t, n, r = s.steps(t, 10.0, max_steps=a.ffs_steps)
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1)
+        cfg = s.config()
+    value = cells * n / (ms / 1e3)
+    return {"deck": f"cases/ffs28.txt layout, 28 blocks of {d.blocks[0].nx}x{d.blocks[0].ny} cells "
+                    f"(refine {a.ffs_refine}), Kn={d.Kn}, {bf.limiter_name(d.limiter)} limiter, "
+                    f"Dirichlet inflow, walls, {sum(c > 0 for blk in d.blocks for c in blk.bc) // 2} block "
+                    "interfaces",
+            "mode": a.mode, "cells": cells, "steps": n, "rejected_attempts": r, "value": value,
+            "unit": "cell-updates/s", "ms_per_step": ms / max(1, n),
+            "per_cell_rate_vs_headline": value / headline if headline else None,
+            "launch": cfg}
+
+
 def adjoint_leg(a, local, stream):
     """The discrete adjoint: J = sum(qx^2 + qy^2) after N Heun steps on 4 blocks of
     n x n cells, gradient wrt the initial temperature field and Kn, checkpoints every
@@ -376,6 +412,9 @@ def main():
                     help="stage-kernel arithmetic: fast (within 1e-10 / 1e-8 of the reference) or exact (bitwise)")
     ap.add_argument("--shard", action="store_true",
                     help="split ONE case over the ranks by block (strong scaling) instead of replicas")
+    ap.add_argument("--ffs-refine", type=int, default=32,
+                    help="refinement of the 28-block forward-facing-step leg (0 = skip)")
+    ap.add_argument("--ffs-steps", type=int, default=100)
     ap.add_argument("--exact-steps", type=int, default=100,
                     help="steps of the bitwise-mode comparison line when --mode fast (0 = skip)")
     a = ap.parse_args()
@@ -493,6 +532,12 @@ def main():
     exact = exact_leg(a, d, scn, local, stream) if (a.mode == "fast" and a.exact_steps > 0) else None
     batched = batched_leg(a, local, stream, rank) if a.batch_cases > 0 else None
     adjoint = adjoint_leg(a, local, stream) if a.adjoint_n > 0 else None
+    ffs = None
+    if a.ffs_refine > 0 and rank == 0:
+        try:
+            ffs = ffs_leg(a, local, stream, value)
+        except Exception as e:       # a leg that fails is reported, not fatal to the line
+            ffs = {"error": str(e)}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -536,6 +581,7 @@ def main():
             "batched": batched,
             "adjoint": adjoint,
             "exact_mode": exact,
+            "many_blocks": ffs,
         }
         print(json.dumps(line), flush=True)
     if dist:
