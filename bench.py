@@ -468,6 +468,7 @@ def main():
     launch = s.config()
     launch["stage2_bulk_tensor_copies"] = s.bulk_copies()
     launch["ghost_fill_in_stage_kernels"] = s.ghost_scatter()
+    launch["programmatic_dependent_launch"] = s.dependent_launch()
     ms = e0.elapsed_time(e1)
     barrier()
     ms_max = ms

@@ -283,6 +283,14 @@ int mbm_config_stage(mbm_ctx *ctx, int heun, double *segment_rows, int *work_ite
  * give the same layers bit for bit. */
 int mbm_ghost_scatter(mbm_ctx *ctx, int *on);
 
+/* *on = 1 when the step loop's kernels (stages, ghost fills, controller) are launched
+ * with programmatic dependent launch: each may be scheduled while the one before it
+ * finishes and waits on the device for its results, which takes the launch gaps out
+ * of the step.  Off with MBM_PDL=0 at context creation, when a stage runs as several
+ * limiter groups on forked streams, and when the step graph cannot be built with it.
+ * No counterpart in the reference. */
+int mbm_dependent_launch(mbm_ctx *ctx, int *on);
+
 /* Host-only: the resolved ghost-cell sources of a block table, 4 ints per ghost
  * cell {dst_block, dst_cell, src, src_block | flags<<16}; cells are J*(nx+6)+I,
  * src < 0 is Dirichlet row -(src+1), flags bit 0/1 = x/y wall sign.  Needs no GPU. */

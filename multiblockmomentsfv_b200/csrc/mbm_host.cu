@@ -135,6 +135,10 @@ struct mbm_ctx {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   bool host_loop = false;           // MBM_HOST_LOOP=1: drive the step loop from the host
+  // the step loop's kernels launched with programmatic dependent launch (MBM_PDL=0: off;
+  // off too when a stage runs as several limiter groups on forked streams, or when the
+  // step graph cannot be built with it)
+  bool pdl = true;
   bool adjoint = false;             // graph body records checkpoints and dt (mbm_params.adjoint)
   bool fast = false;                // MBM_MODE_FAST: the fastmath stage kernel
   // a case split over ranks by block (mbm_create_sharded)
@@ -503,6 +507,10 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
 // the body of one step attempt: stage 1, fill TMP, stage 2, fill NEW, controller (the
 // fills inside the stage kernels when they scatter them)
 static cudaError_t launch_attempt(mbm_ctx* c, cudaGraphConditionalHandle h, int use_handle) {
+  struct PdlScope {              // the attempt's launches use it; the thread's others do not
+    explicit PdlScope(bool on) { tl_pdl = on; }
+    ~PdlScope() { tl_pdl = false; }
+  } pdl_scope(c->pdl && c->groups[0].size() <= 1 && c->groups[1].size() <= 1);
   cudaError_t e;
   const bool g = !c->gscatter;
   if ((e = launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP, 0, nullptr, true))) return e;
@@ -984,23 +992,41 @@ static int create_impl(const std::vector<mbm_block_desc>& glob, const std::vecto
 
   // the step loop: while (any case live) { stage 1; fill TMP; stage 2; fill NEW; control }
   {
-    cudaGraphConditionalHandle h;
-    CKC(cudaGraphCreate(&c->graph, 0));
-    CKC(cudaGraphConditionalHandleCreate(&h, c->graph, 1, cudaGraphCondAssignDefault));
-    cudaGraphNodeParams np = {};
-    np.type = cudaGraphNodeTypeConditional;
-    np.conditional.handle = h;
-    np.conditional.type = cudaGraphCondTypeWhile;
-    np.conditional.size = 1;
-    cudaGraphNode_t node;
-    CKC(cudaGraphAddNode(&node, c->graph, nullptr, 0, &np));
-    cudaGraph_t body = np.conditional.phGraph_out[0];
-    CKC(cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e1 = launch_attempt(c, h, 1);
-    cudaGraph_t captured = nullptr;
-    CKC(cudaStreamEndCapture(c->stream, &captured));
-    CKC(e1);
-    CKC(cudaGraphInstantiate(&c->gexec, c->graph, 0));
+    const char* pe = getenv("MBM_PDL");
+    c->pdl = !(pe && atoi(pe) == 0);
+    auto build_graph = [&]() -> cudaError_t {
+      cudaError_t e;
+      cudaGraphConditionalHandle h;
+      if ((e = cudaGraphCreate(&c->graph, 0))) return e;
+      if ((e = cudaGraphConditionalHandleCreate(&h, c->graph, 1, cudaGraphCondAssignDefault))) return e;
+      cudaGraphNodeParams np = {};
+      np.type = cudaGraphNodeTypeConditional;
+      np.conditional.handle = h;
+      np.conditional.type = cudaGraphCondTypeWhile;
+      np.conditional.size = 1;
+      cudaGraphNode_t node;
+      if ((e = cudaGraphAddNode(&node, c->graph, nullptr, 0, &np))) return e;
+      cudaGraph_t body = np.conditional.phGraph_out[0];
+      if ((e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)))
+        return e;
+      const cudaError_t e1 = launch_attempt(c, h, 1);
+      cudaGraph_t captured = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(c->stream, &captured);
+      if (e1) return e1;
+      if (e2) return e2;
+      return cudaGraphInstantiate(&c->gexec, c->graph, 0);
+    };
+    cudaError_t eg = build_graph();
+    if (eg != cudaSuccess && c->pdl) {   // without programmatic launches, once more
+      if (c->gexec) cudaGraphExecDestroy(c->gexec);
+      if (c->graph) cudaGraphDestroy(c->graph);
+      c->gexec = nullptr;
+      c->graph = nullptr;
+      cudaGetLastError();
+      c->pdl = false;
+      eg = build_graph();
+    }
+    CKC(eg);
   }
   int st = wait_stream(c);
   if (st != MBM_OK) return bail(st);
@@ -1361,6 +1387,12 @@ extern "C" int mbm_bulk_copies(mbm_ctx* c, int* on) {
   if (!c || !on) return fail(c, MBM_EINVAL, "mbm_bulk_copies: bad argument");
   *on = c->dtmap != nullptr;
   if (!c->dtmap && !c->tma_note.empty()) c->err = c->tma_note;
+  return MBM_OK;
+}
+
+extern "C" int mbm_dependent_launch(mbm_ctx* c, int* on) {
+  if (!c || !on) return fail(c, MBM_EINVAL, "mbm_dependent_launch: bad argument");
+  *on = c->pdl && c->groups[0].size() <= 1 && c->groups[1].size() <= 1 ? 1 : 0;
   return MBM_OK;
 }
 

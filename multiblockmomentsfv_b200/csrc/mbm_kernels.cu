@@ -12,6 +12,8 @@
 
 namespace mbm {
 
+thread_local bool tl_pdl = false;
+
 using namespace bitwise;    // the output conversion uses the bitwise Primitive
 
 // ---------------------------------------------------------------- ghost fill --
@@ -22,6 +24,7 @@ __global__ void ghost_kernel(const BlockDev* __restrict__ blk, const CaseDev* __
                              const GhostEntry* __restrict__ map, int n, double* buf0,
                              double* buf1, double* buf2, const double* __restrict__ dirichlet,
                              const double* __restrict__ recv, int sel) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const GhostEntry e = map[i];
@@ -56,6 +59,7 @@ __global__ void ghost_kernel(const BlockDev* __restrict__ blk, const CaseDev* __
 __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __restrict__ blk,
                                unsigned long long* lam, double* trace, int* queues,
                                cudaGraphConditionalHandle h, int use_handle, const double* cfl_ext) {
+  pdl_enter();
   if (threadIdx.x < 10) queues[threadIdx.x] = 0;  // work counters [stage][limiter]
   int live = 0;
   for (int c = threadIdx.x; c < ncases; c += blockDim.x) {
@@ -119,6 +123,7 @@ __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __res
 // rejected attempt copies the same DATA again
 __global__ void ckpt_kernel(const CaseDev* __restrict__ cases, const double* buf0, const double* buf1,
                             long long layer_elems) {
+  pdl_enter();
   const CaseDev& cs = cases[0];
   if (!cs.ckpt || cs.ckpt_every <= 0 || cs.nstep == 0 || cs.nstep % cs.ckpt_every) return;
   const double* src = cs.cur ? buf1 : buf0;
@@ -130,7 +135,7 @@ __global__ void ckpt_kernel(const CaseDev* __restrict__ cases, const double* buf
 
 cudaError_t launch_ckpt(const CaseDev* cases, const double* buf0, const double* buf1, long long layer_elems,
                         int grid, cudaStream_t s) {
-  ckpt_kernel<<<grid, 256, 0, s>>>(cases, buf0, buf1, layer_elems);
+  return launch_k(ckpt_kernel, dim3(grid), dim3(256), 0, s, cases, buf0, buf1, layer_elems);
   return cudaGetLastError();
 }
 
@@ -343,16 +348,15 @@ cudaError_t launch_ghost(const BlockDev* blk, const CaseDev* cases, const GhostE
                          double* const buf[3], const double* dirichlet, int sel, cudaStream_t s,
                          const double* recv) {
   if (n <= 0) return cudaSuccess;
-  ghost_kernel<<<(n + 127) / 128, 128, 0, s>>>(blk, cases, map, n, buf[0], buf[1], buf[2],
-                                               dirichlet, recv, sel);
-  return cudaGetLastError();
+  return launch_k(ghost_kernel, dim3((n + 127) / 128), dim3(128), 0, s, blk, (const CaseDev*)cases, map, n, buf[0],
+                  buf[1], buf[2], dirichlet, recv, sel);
 }
 
 cudaError_t launch_control(CaseDev* cases, int ncases, const BlockDev* blk, unsigned long long* lam,
                            double* trace, int* queues, cudaGraphConditionalHandle h, int use_handle,
                            cudaStream_t s) {
-  control_kernel<<<1, 256, 0, s>>>(cases, ncases, blk, lam, trace, queues, h, use_handle, nullptr);
-  return cudaGetLastError();
+  return launch_k(control_kernel, dim3(1), dim3(256), 0, s, cases, ncases, blk, lam, trace, queues, h, use_handle,
+                  (const double*)nullptr);
 }
 
 cudaError_t launch_stage_cfl(const BlockDev* blk, int nblk, const CaseDev* cases,

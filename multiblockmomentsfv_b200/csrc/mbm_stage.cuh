@@ -618,6 +618,7 @@ constexpr int stage_smem() { return (int)sizeof(WarpWindow<HEUN>) * STAGE_WARPS;
 #endif
 template <int HEUN, int LIM, bool TMA>
 __global__ void STAGE_BOUNDS stage_kernel(const StageArgs a) {
+  pdl_enter();
   extern __shared__ __align__(128) unsigned char stage_shared[];
   WarpWindow<HEUN>* win = reinterpret_cast<WarpWindow<HEUN>*>(stage_shared);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -691,13 +692,12 @@ int stage_cta_warps() { return STAGE_WARPS; }
 template <int HEUN, bool TMA>
 static cudaError_t launch_stage_lim(int lim, const StageArgs& a, int grid, cudaStream_t s) {
   switch (lim) {
-    case 0: stage_kernel<HEUN, 0, TMA><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
-    case 1: stage_kernel<HEUN, 1, TMA><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
-    case 2: stage_kernel<HEUN, 2, TMA><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
-    case 3: stage_kernel<HEUN, 3, TMA><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
-    default: stage_kernel<HEUN, 4, TMA><<<grid, 32 * STAGE_WARPS, stage_smem<HEUN>(), s>>>(a); break;
+    case 0: return launch_k(stage_kernel<HEUN, 0, TMA>, dim3(grid), dim3(32 * STAGE_WARPS), stage_smem<HEUN>(), s, a);
+    case 1: return launch_k(stage_kernel<HEUN, 1, TMA>, dim3(grid), dim3(32 * STAGE_WARPS), stage_smem<HEUN>(), s, a);
+    case 2: return launch_k(stage_kernel<HEUN, 2, TMA>, dim3(grid), dim3(32 * STAGE_WARPS), stage_smem<HEUN>(), s, a);
+    case 3: return launch_k(stage_kernel<HEUN, 3, TMA>, dim3(grid), dim3(32 * STAGE_WARPS), stage_smem<HEUN>(), s, a);
+    default: return launch_k(stage_kernel<HEUN, 4, TMA>, dim3(grid), dim3(32 * STAGE_WARPS), stage_smem<HEUN>(), s, a);
   }
-  return cudaGetLastError();
 }
 
 cudaError_t launch_stage(int lim, const StageArgs& a, int grid, cudaStream_t s) {

@@ -197,6 +197,12 @@ class Solver:
         self._check(self.L.mbm_bulk_copies(self.ctx, C.byref(on)))
         return bool(on.value)
 
+    def dependent_launch(self) -> bool:
+        """Whether the step loop's kernels use programmatic dependent launch."""
+        on = C.c_int(0)
+        self._check(self.L.mbm_dependent_launch(self.ctx, C.byref(on)))
+        return bool(on.value)
+
     def ghost_scatter(self) -> bool:
         """Whether the step loop's ghost fills are done inside the stage kernels."""
         on = C.c_int(0)
