@@ -58,6 +58,7 @@ __device__ __forceinline__ void load9(const double* base, const BlockDev& B, int
 
 // pass A: the forward stage's projected primitives (Aux.Prim, src/Main.c:314-336)
 __global__ void adj_prims(AdjArgs a, long long nthr) {
+  pdl_enter();
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, J;
   if (k >= nthr || !locate(a.blk, a.nblk, k, b, I, J)) return;
@@ -143,6 +144,7 @@ __device__ __forceinline__ void face_adj(const AdjArgs& a, const BlockDev& B, in
 template <int HEUN, int LIM>
 __global__ void __launch_bounds__(128, ADJ_FACE_CTAS) adj_faces(AdjArgs a, long long nthr, double* FLx, double* FRx,
                                                     double* FLy, double* FRy) {
+  pdl_enter();
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, J;
   if (k >= nthr || !locate(a.blk, a.nblk, k, b, I, J)) return;
@@ -263,6 +265,7 @@ __device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, 
 template <int HEUN, int LIM>
 __global__ void __launch_bounds__(128, ADJ_CELL_CTAS) adj_cells(AdjArgs a, long long nthr, const double* FLx,
                                                     const double* FRx, const double* FLy, const double* FRy) {
+  pdl_enter();
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, J;
   double knb = 0.0;
@@ -278,6 +281,7 @@ __global__ void __launch_bounds__(128, ADJ_CELL_CTAS) adj_cells(AdjArgs a, long 
 // adjoint of the ghost fill: ghost adjoint -> its source cell (wall signs), then
 // zero; one thread per (ghost cell, component)
 __global__ void adj_ghosts(const BlockDev* __restrict__ blk, const GhostEntry* __restrict__ map, int n, double* l) {
+  pdl_enter();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)n * NV) return;
   const int i = (int)(t / NV), m = (int)(t - (long long)i * NV);
@@ -606,8 +610,9 @@ cudaError_t adjoint_stage_march(const AdjArgs& a, int grid, cudaStream_t s) {
 template <int HEUN, int LIM>
 static void faces_cells(const AdjArgs& a0, long long nthr, unsigned G, double* FLx, double* FRx, double* FLy,
                         double* FRy, cudaStream_t s) {
-  adj_faces<HEUN, LIM><<<G, 128, 0, s>>>(a0, nthr, FLx, FRx, FLy, FRy);
-  adj_cells<HEUN, LIM><<<G, 128, 0, s>>>(a0, nthr, FLx, FRx, FLy, FRy);
+  launch_k(adj_faces<HEUN, LIM>, dim3(G), dim3(128), 0, s, a0, nthr, FLx, FRx, FLy, FRy);
+  launch_k(adj_cells<HEUN, LIM>, dim3(G), dim3(128), 0, s, a0, nthr, (const double*)FLx, (const double*)FRx,
+           (const double*)FLy, (const double*)FRy);
 }
 
 template <int HEUN>
@@ -626,7 +631,7 @@ cudaError_t adjoint_stage(const AdjArgs& a0, long long nthr, double* FLx, double
                           double* FRy, cudaStream_t s) {
   const int T = 128;
   const unsigned G = (unsigned)(nthr / T);
-  adj_prims<<<G, T, 0, s>>>(a0, nthr);
+  launch_k(adj_prims, dim3(G), dim3(T), 0, s, a0, nthr);
   if (a0.heun) faces_cells_lim<1>(a0, nthr, G, FLx, FRx, FLy, FRy, s);
   else faces_cells_lim<0>(a0, nthr, G, FLx, FRx, FLy, FRy, s);
   return cudaGetLastError();
@@ -634,7 +639,7 @@ cudaError_t adjoint_stage(const AdjArgs& a0, long long nthr, double* FLx, double
 
 cudaError_t adjoint_ghosts(const BlockDev* blk, const GhostEntry* map, int n, double* l, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  adj_ghosts<<<(unsigned)(((long long)n * NV + 255) / 256), 256, 0, s>>>(blk, map, n, l);
+  launch_k(adj_ghosts, dim3((unsigned)(((long long)n * NV + 255) / 256)), dim3(256), 0, s, blk, map, n, l);
   return cudaGetLastError();
 }
 

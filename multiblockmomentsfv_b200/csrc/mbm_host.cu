@@ -1574,6 +1574,10 @@ static int frozen_step(mbm_ctx* c, const double* in, double* out, const double* 
 // reverse of one step: lam (adjoint of D_{n+1}, interior) -> lam_next (adjoint of
 // D_n); Tn = stage 1 of D_n with its ghost fill
 static int adj_step(mbm_ctx* c, const double* Dn, const double* Tn, double dt, double* lam, double* lam_next) {
+  struct PdlScope {              // the three-pass kernels wait on the device for the one before
+    explicit PdlScope(bool on) { tl_pdl = on; }
+    ~PdlScope() { tl_pdl = false; }
+  } pdl_scope(c->pdl && !c->adj_march);
   double* lamT = c->adj_buf[2];
   double* P = c->adj_buf[3];
   const long long nc = adj_threads(c);
