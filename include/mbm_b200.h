@@ -336,7 +336,8 @@ int mbm_stage_noalloc(const mbm_block_desc *blocks, int nblocks, const double *i
  * CFLmax 1, CFLreg as given) recording every dt and a checkpoint every `every`
  * steps; evaluate J = sum over interior cells of qx^2 + qy^2 of the final state;
  * then sweep back through the steps with dt frozen, recomputing each segment from
- * its checkpoint, through the hand-written reverse of Update (relaxation, HLL
+ * its checkpoint (the last segment's states are kept by the forward run instead;
+ * MBM_ADJ_TAIL=0 recomputes it too), through the hand-written reverse of Update (relaxation, HLL
  * fluxes, limiters with one-sided derivatives at kinks) and of SetBoundary.
  * grad (host, may be NULL) receives dJ/du0 in the layer layout of mbm_upload
  * (ghost cells zero), *grad_Kn = dJ/dKn, dts[nsteps] (may be NULL) the frozen dt

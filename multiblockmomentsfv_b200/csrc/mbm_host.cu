@@ -43,8 +43,8 @@ cudaError_t launch_control_ext(CaseDev* cases, const BlockDev* blk, unsigned lon
 cudaError_t launch_control(CaseDev* cases, int ncases, const BlockDev* blk, unsigned long long* lam,
                            double* trace, int* queues, cudaGraphConditionalHandle h, int use_handle,
                            cudaStream_t s);
-cudaError_t launch_ckpt(const CaseDev* cases, const double* buf0, const double* buf1, long long layer_elems,
-                        int grid, cudaStream_t s);
+cudaError_t launch_ckpt(const CaseDev* cases, const double* buf0, const double* buf1, const double* buf2,
+                        long long layer_elems, int grid, cudaStream_t s);
 cudaError_t adjoint_stage(const AdjArgs& a0, long long ncell, double* FLx, double* FRx, double* FLy,
                           double* FRy, cudaStream_t s);
 cudaError_t adjoint_ghosts(const BlockDev* blk, const GhostEntry* map, int n, double* l, cudaStream_t s);
@@ -519,7 +519,7 @@ static cudaError_t launch_attempt(mbm_ctx* c, cudaGraphConditionalHandle h, int 
   if (g && (e = launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, c->buf, c->ddir, SEL_OTHER, c->stream))) return e;
   if ((e = launch_control(c->dcase, c->ncase, c->dblk, c->dlam, c->dtrace, c->dqueue, h, use_handle, c->stream)))
     return e;
-  if (c->adjoint) return launch_ckpt(c->dcase, c->buf[0], c->buf[1], c->layer_elems, 4 * c->nsm, c->stream);
+  if (c->adjoint) return launch_ckpt(c->dcase, c->buf[0], c->buf[1], c->buf[2], c->layer_elems, 4 * c->nsm, c->stream);
   return cudaSuccess;
 }
 
@@ -1649,18 +1649,33 @@ extern "C" int mbm_adjoint_run(mbm_ctx* c, double* t, int nsteps, int every, dou
   CK(cudaEventCreate(&e2));
   // forward: Steps with a step cap, recording dt and checkpoints (step 0 = the input state)
   CaseDev& h = c->hcase[0];
+  // the last segment [tail_a, nsteps) is kept by the forward run itself (into the segment
+  // buffers the reverse sweep reads first), so the sweep starts without recomputing it
+  // (MBM_ADJ_TAIL=0: recomputed like the others)
+  const char* te = getenv("MBM_ADJ_TAIL");
+  const bool keep_tail = !(te && atoi(te) == 0);
+  const int tail_seg = (nsteps - 1) / every, tail_buf = tail_seg & 1;
+  CK(cudaEventRecord(e0, c->stream));
   CK(cudaMemcpyAsync(c->adj_ckpt, c->buf[h.cur], bytes, cudaMemcpyDeviceToDevice, c->stream));
   h.ckpt = c->adj_ckpt;
   h.ckpt_every = every;
   h.dtlog = c->adj_dtlog;
   h.dtlog_cap = nsteps;
-  CK(cudaEventRecord(e0, c->stream));
+  if (keep_tail) {
+    h.tail_a = tail_seg * every;
+    h.tail_b = nsteps;
+    h.tail_d = c->adj_seg[tail_buf];
+    h.tail_t = c->adj_segT[tail_buf];
+    if (h.tail_a == 0) CK(cudaMemcpyAsync(h.tail_d, c->buf[h.cur], bytes, cudaMemcpyDeviceToDevice, c->stream));
+  }
   int n = 0, r = 0;
   st = mbm_steps_capped(c, t, 1e300, 1.0, CFLreg, nsteps, &n, &r);
   h.ckpt = nullptr;
   h.dtlog = nullptr;
   h.ckpt_every = 0;
   h.dtlog_cap = 0;
+  h.tail_d = h.tail_t = nullptr;
+  h.tail_a = h.tail_b = 0;
   if (st) return st;
   if ((st = push_cases(c))) return st;
   CK(cudaEventRecord(e1, c->stream));
@@ -1708,7 +1723,12 @@ extern "C" int mbm_adjoint_run(mbm_ctx* c, double* t, int nsteps, int every, dou
     return rc;
   };
   const int nseg = (n - 1) / every + 1;
-  if ((st = recompute(nseg - 1))) return fail(c, st, "mbm_adjoint_run: recomputation failed");
+  if (keep_tail && n == nsteps) {      // the forward run kept the last segment
+    CK(cudaEventRecord(c->adj_ready[tail_buf], c->stream));
+    used[tail_buf] = true;
+  } else if ((st = recompute(nseg - 1))) {
+    return fail(c, st, "mbm_adjoint_run: recomputation failed");
+  }
   for (int sg = nseg - 1; sg >= 0; sg--) {
     const int a = sg * every, b = std::min(n, a + every), k2 = sg & 1;
     if (sg > 0 && (st = recompute(sg - 1))) return fail(c, st, "mbm_adjoint_run: recomputation failed");

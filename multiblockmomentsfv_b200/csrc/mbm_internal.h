@@ -75,6 +75,12 @@ struct CaseDev {       // per-case step controller (src/Main.c:189-244)
   int dtlog_cap;       // accepted dt values recorded into dtlog (adjoint runs)
   double* dtlog;
   double* ckpt;        // checkpoint layers (layer_elems doubles each)
+  int accepted;        // the controller accepted the attempt just made
+  // adjoint runs: the states D_a .. D_{b-1} and stage-1 states T_a .. T_{b-1} of the last
+  // checkpoint segment [a, b), kept as the forward run makes them (not null: on)
+  int tail_a, tail_b;
+  double* tail_d;
+  double* tail_t;
 };
 
 struct StageArgs {

@@ -82,6 +82,7 @@ __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __res
     const double cfl = cfl_ext ? *cfl_ext : rmax(cfl1, rmax(cfl2, 0.0));
     cs.cfl_last = cfl;
     cs.attempts++;
+    cs.accepted = 0;
     if (cs.nonfinite) {       // a stage wrote a NaN or infinity: stop before accepting it
       // bit 2: a bounded wait for a bulk copy ran out (MBM_ETIMEOUT), else MBM_ENONFINITE
       cs.status = (cs.nonfinite & 2) ? 3 : 2;
@@ -96,6 +97,7 @@ __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __res
       cs.dt = nd;
       cs.nstep++;
       cs.cur = 1 - cs.cur;
+      cs.accepted = 1;
       if (cs.dtlog && cs.nstep <= cs.dtlog_cap) cs.dtlog[cs.nstep - 1] = dt;   // frozen for the adjoint
       if (cs.show_every > 0 && cs.nstep % cs.show_every == 0 && cs.trace_n < MAX_TRACE) {
         double* r = trace + ((size_t)c * MAX_TRACE + cs.trace_n) * 4;
@@ -120,22 +122,35 @@ __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __res
 }
 
 // checkpoint of DATA after every ckpt_every-th accepted step (adjoint runs); a
-// rejected attempt copies the same DATA again
+// rejected attempt copies the same DATA again.  After an accepted step m inside the last
+// segment [a, b) it also keeps that step's stage-1 state (TMP, still the accepted
+// attempt's) and the new state D_m, so that the reverse sweep need not recompute the
+// segment.
 __global__ void ckpt_kernel(const CaseDev* __restrict__ cases, const double* buf0, const double* buf1,
-                            long long layer_elems) {
+                            const double* buf2, long long layer_elems) {
   pdl_enter();
   const CaseDev& cs = cases[0];
+  const long long k0 = (long long)blockIdx.x * blockDim.x + threadIdx.x, ks = (long long)gridDim.x * blockDim.x;
+  const double* data = cs.cur ? buf1 : buf0;
+  if (cs.tail_d && cs.accepted) {
+    const int m = cs.nstep;   // step m-1 was just accepted: T_{m-1} in TMP, D_m in DATA
+    if (m - 1 >= cs.tail_a && m - 1 < cs.tail_b) {
+      double* dst = cs.tail_t + (size_t)(m - 1 - cs.tail_a) * layer_elems;
+      for (long long k = k0; k < layer_elems; k += ks) dst[k] = buf2[k];
+    }
+    if (m >= cs.tail_a && m < cs.tail_b) {
+      double* dst = cs.tail_d + (size_t)(m - cs.tail_a) * layer_elems;
+      for (long long k = k0; k < layer_elems; k += ks) dst[k] = data[k];
+    }
+  }
   if (!cs.ckpt || cs.ckpt_every <= 0 || cs.nstep == 0 || cs.nstep % cs.ckpt_every) return;
-  const double* src = cs.cur ? buf1 : buf0;
   double* dst = cs.ckpt + (size_t)(cs.nstep / cs.ckpt_every) * layer_elems;
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < layer_elems;
-       k += (long long)gridDim.x * blockDim.x)
-    dst[k] = src[k];
+  for (long long k = k0; k < layer_elems; k += ks) dst[k] = data[k];
 }
 
-cudaError_t launch_ckpt(const CaseDev* cases, const double* buf0, const double* buf1, long long layer_elems,
-                        int grid, cudaStream_t s) {
-  return launch_k(ckpt_kernel, dim3(grid), dim3(256), 0, s, cases, buf0, buf1, layer_elems);
+cudaError_t launch_ckpt(const CaseDev* cases, const double* buf0, const double* buf1, const double* buf2,
+                        long long layer_elems, int grid, cudaStream_t s) {
+  return launch_k(ckpt_kernel, dim3(grid), dim3(256), 0, s, cases, buf0, buf1, buf2, layer_elems);
   return cudaGetLastError();
 }
 

@@ -307,6 +307,33 @@ def test_row_march_equals_three_pass(limiter):
     assert abs(k1 - k0) <= 1e-11 * abs(k0)
 
 
+@pytest.mark.parametrize("nsteps,every", [(16, 5), (12, 4), (3, 5)])
+def test_tail_segment_kept_by_forward(nsteps, every):
+    """The forward run keeps the last checkpoint segment's states for the reverse sweep
+    (the default) or the sweep recomputes it (MBM_ADJ_TAIL=0): the same gradient, for a
+    partial last segment, a full one, and a run shorter than one segment."""
+    import os
+    d = H.quadrant_deck(32, Kn=0.01, limiter=bf.LIM_HARMONIC)
+    base = adj.smooth_base(d, 23)
+    th0 = _theta0(d, np.random.default_rng(23))
+    out = {}
+    for tail in ("1", "0"):
+        os.environ["MBM_ADJ_TAIL"] = tail
+        try:
+            with adj.Sensitivity(d, base, mode="fast") as S:
+                S.load(adj.state_from_theta(d, base, th0))
+                J, g, gK, dts, ms = S.run(nsteps, every)
+                out[tail] = (J, np.concatenate([x.ravel() for x in g]), gK, dts)
+        finally:
+            del os.environ["MBM_ADJ_TAIL"]
+    (J1, g1, k1, d1), (J0, g0, k0, d0) = out["1"], out["0"]
+    assert J1 == J0
+    H.assert_bitwise(d1, d0, "dt")
+    scale = np.abs(g0).max()
+    assert np.abs(g1 - g0).max() <= 1e-12 * scale, np.abs(g1 - g0).max() / scale
+    assert abs(k1 - k0) <= 1e-12 * abs(k0)
+
+
 def test_replay_before_the_first_adjoint_run():
     """A context whose first call is mbm_replay (which makes only the adjoint layer it
     needs) runs the adjoint afterwards with the same result as a context that runs it
