@@ -331,10 +331,18 @@ int mbm_stage_noalloc(const mbm_block_desc *blocks, int nblocks, const double *i
                       const double *data0, double *out, double Kn, double F, int limiter,
                       double dt, int heun, double *cfl, void *stream);
 
+/* The scalar functional of the final state the adjoint differentiates, summed over
+ * interior cells (unweighted): the heat flux q1^2 + q2^2 (the default), the temperature
+ * theta, or the deviatoric temperature tensor (T11 - theta)^2 + 2 T12^2 + (T22 - theta)^2.
+ * No counterpart in the reference. */
+enum { MBM_J_HEAT_FLUX = 0, MBM_J_TEMPERATURE = 1, MBM_J_DEVIATORIC = 2 };
+int mbm_set_functional(mbm_ctx *ctx, int kind);
+
 /* Discrete adjoint (no counterpart in the reference): from the current DATA (the
  * initial state u0), run Steps for `nsteps` accepted steps (dt restarts at 1e-4,
  * CFLmax 1, CFLreg as given) recording every dt and a checkpoint every `every`
- * steps; evaluate J = sum over interior cells of qx^2 + qy^2 of the final state;
+ * steps; evaluate J (mbm_set_functional; by default the sum over interior cells of
+ * qx^2 + qy^2) of the final state;
  * then sweep back through the steps with dt frozen, recomputing each segment from
  * its checkpoint (the last segment's states are kept by the forward run instead;
  * MBM_ADJ_TAIL=0 recomputes it too), through the hand-written reverse of Update (relaxation, HLL
@@ -351,7 +359,7 @@ int mbm_adjoint_run(mbm_ctx *ctx, double *t, int nsteps, int every, double CFLre
                     double *grad, double *grad_Kn, double *dts, double *ms);
 
 /* Frozen-dt forward: n Heun steps of DATA with the given dt values (no controller,
- * as the adjoint sees the run); *J (may be NULL) = the heat-flux functional above. */
+ * as the adjoint sees the run); *J (may be NULL) = the functional above. */
 int mbm_replay(mbm_ctx *ctx, const double *dts, int n, double *J);
 
 /* Kn and body force F of every case (the reference's globals Kn, F). */

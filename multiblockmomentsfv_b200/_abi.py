@@ -21,7 +21,7 @@ EXPORTS = (
     "mbm_create", "mbm_destroy", "mbm_upload", "mbm_download", "mbm_set_dirichlet",
     "mbm_set_boundary", "mbm_update", "mbm_time_update", "mbm_steps", "mbm_steps_capped",
     "mbm_time_stage", "mbm_trace", "mbm_attempts", "mbm_case_status", "mbm_config",
-    "mbm_create_batch", "mbm_steps_batch", "mbm_trace_case", "mbm_stage_noalloc", "mbm_bulk_copies", "mbm_load_fields", "mbm_config_stage", "mbm_ghost_scatter", "mbm_dependent_launch",
+    "mbm_create_batch", "mbm_steps_batch", "mbm_trace_case", "mbm_stage_noalloc", "mbm_bulk_copies", "mbm_load_fields", "mbm_config_stage", "mbm_ghost_scatter", "mbm_dependent_launch", "mbm_set_functional",
     "mbm_adjoint_run", "mbm_replay", "mbm_set_physics", "mbm_output_fields",
     "mbm_ghost_map", "mbm_strerror", "mbm_last_error", "mbm_version",
     "mbm_shard_plan", "mbm_create_sharded", "mbm_shard_buffers", "mbm_shard_set_dirichlet",
@@ -112,6 +112,7 @@ def lib(path: str = None):
     L.mbm_adjoint_run.argtypes = [vp, dp, C.c_int, C.c_int, C.c_double, dp, dp, dp, dp, dp]
     L.mbm_replay.argtypes = [vp, dp, C.c_int, dp]
     L.mbm_set_physics.argtypes = [vp, C.c_double, C.c_double]
+    L.mbm_set_functional.argtypes = [vp, C.c_int]
     L.mbm_dependent_launch.argtypes = [vp, P(C.c_int)]
     L.mbm_ghost_scatter.argtypes = [vp, P(C.c_int)]
     L.mbm_config_stage.argtypes = [vp, C.c_int, dp, P(C.c_int), P(C.c_int)]

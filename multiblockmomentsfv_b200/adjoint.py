@@ -1,8 +1,10 @@
 """Sensitivities of the Heun path: the discrete adjoint (mbm_adjoint_run) and a
 thin torch.autograd.Function over it.
 
-The functional is J = sum over interior cells of qx^2 + qy^2 of the state after N
-Heun steps (the squared, unweighted l2 norm of the final heat flux).  The
+The functional is, by default, J = sum over interior cells of qx^2 + qy^2 of the
+state after N Heun steps (the squared, unweighted l2 norm of the final heat flux);
+`functional` selects the sum of theta or of the deviatoric temperature tensor's
+squares (T11 - theta)^2 + 2 T12^2 + (T22 - theta)^2 instead.  The
 parameters are the initial temperature field theta0 (one value per interior cell;
 density and velocity fixed, T_ij = theta0 delta_ij, q = 0 as in SetInitial,
 src/Scenario.c:140-152) and the Knudsen number.  dt is frozen from the forward run:
@@ -33,7 +35,11 @@ def _bind(L):
     L.mbm_adjoint_run.argtypes = [C.c_void_p, dp, C.c_int, C.c_int, C.c_double, dp, dp, dp, dp, dp]
     L.mbm_replay.argtypes = [C.c_void_p, dp, C.c_int, dp]
     L.mbm_set_physics.argtypes = [C.c_void_p, C.c_double, C.c_double]
+    L.mbm_set_functional.argtypes = [C.c_void_p, C.c_int]
     return L
+
+
+FUNCTIONALS = {"heat_flux": 0, "temperature": 1, "deviatoric": 2}
 
 
 def state_from_theta(deck: bf.Deck, base: Sequence[np.ndarray], theta0: Sequence[np.ndarray]) -> List[np.ndarray]:
@@ -85,11 +91,12 @@ class Sensitivity:
     density and velocity of the initial states (padded moment layers)."""
 
     def __init__(self, deck: bf.Deck, base: Sequence[np.ndarray], device: int = 0, stream=None,
-                 scenario: Optional[sc.Scenario] = None, mode: str = "exact"):
+                 scenario: Optional[sc.Scenario] = None, mode: str = "exact", functional: str = "heat_flux"):
         self.deck = deck
         self.base = list(base)
         self.s = sv.Solver(deck, scenario, device=device, show_every=0, stream=stream, adjoint=True, mode=mode)
         self.L = _bind(self.s.L)
+        _abi.check(self.L.mbm_set_functional(self.s.ctx, FUNCTIONALS[functional]), self.s.ctx)
 
     def close(self):
         self.s.close()

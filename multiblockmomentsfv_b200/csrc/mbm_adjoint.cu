@@ -298,11 +298,14 @@ __global__ void adj_ghosts(const BlockDev* __restrict__ blk, const GhostEntry* _
   atomicAdd(l + S.off + e.src + m * S.plane, flip ? -v : v);
 }
 
-// dJ/dU of J = sum over interior cells of q1^2 + q2^2 (heat flux of the final state);
+// J = sum over interior cells of f(P) of the final state, and dJ/dU; f by `kind`:
+//   0  q1^2 + q2^2                                (heat flux)
+//   1  theta                                      (temperature)
+//   2  (T11 - theta)^2 + 2 T12^2 + (T22 - theta)^2 (deviatoric temperature tensor)
 // each CTA writes its partial sum (fixed order: warp shuffles, then the warps in
 // order), so J does not depend on scheduling and finite differences of it are clean
 __global__ void adj_functional(const BlockDev* __restrict__ blk, int nblk, const double* x, double* l,
-                               long long nthr, double* part) {
+                               long long nthr, double* part, int kind) {
   __shared__ double ws[4];
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int b, I, Jj;
@@ -313,9 +316,21 @@ __global__ void adj_functional(const BlockDev* __restrict__ blk, int nblk, const
       double U[NV], P[NV], Pb[NV] = {0}, Ub[NV] = {0};
       load9(x, B, I, Jj, U);
       mbm_adj::prim(U, P);
-      jv = P[7] * P[7] + P[8] * P[8];
-      Pb[7] = 2 * P[7];
-      Pb[8] = 2 * P[8];
+      if (kind == 1) {
+        jv = P[3];
+        Pb[3] = 1.0;
+      } else if (kind == 2) {
+        const double s11 = P[4] - P[3], s22 = P[6] - P[3];
+        jv = s11 * s11 + 2 * P[5] * P[5] + s22 * s22;
+        Pb[4] = 2 * s11;
+        Pb[5] = 4 * P[5];
+        Pb[6] = 2 * s22;
+        Pb[3] = -2 * (s11 + s22);
+      } else {
+        jv = P[7] * P[7] + P[8] * P[8];
+        Pb[7] = 2 * P[7];
+        Pb[8] = 2 * P[8];
+      }
       mbm_adj::prim_adj(U, Pb, Ub);
       const long long i = cidx(B, I, Jj);
       for (int m = 0; m < NV; m++) l[i + m * B.plane] = Ub[m];
@@ -645,9 +660,9 @@ cudaError_t adjoint_ghosts(const BlockDev* blk, const GhostEntry* map, int n, do
 
 // nthr: 128 threads per 32 x 4 tile of every block; part: nthr / 128 doubles of scratch
 cudaError_t adjoint_functional(const BlockDev* blk, int nblk, const double* x, double* l, long long nthr,
-                               double* part, double* J, cudaStream_t s) {
+                               double* part, double* J, int kind, cudaStream_t s) {
   const unsigned G = (unsigned)(nthr / 128);
-  adj_functional<<<G, 128, 0, s>>>(blk, nblk, x, l, nthr, part);
+  adj_functional<<<G, 128, 0, s>>>(blk, nblk, x, l, nthr, part, kind);
   sum_partials<<<1, 256, 0, s>>>(part, (int)G, J);
   return cudaGetLastError();
 }

@@ -51,7 +51,7 @@ cudaError_t adjoint_ghosts(const BlockDev* blk, const GhostEntry* map, int n, do
 cudaError_t adjoint_stage_march(const AdjArgs& a, int grid, cudaStream_t s);
 int adjoint_march_ctas();
 cudaError_t adjoint_functional(const BlockDev* blk, int nblk, const double* x, double* l, long long ncell,
-                               double* part, double* J, cudaStream_t s);
+                               double* part, double* J, int kind, cudaStream_t s);
 cudaError_t launch_fill_uniform(double* base, long long plane, cudaStream_t s);
 cudaError_t launch_stage_cfl(const BlockDev* blk, int nblk, const CaseDev* cases,
                              unsigned long long* lam, int stage, double* out, cudaStream_t s);
@@ -168,6 +168,7 @@ struct mbm_ctx {
   int adj_nwork = 0, adj_grid = 0;
   int* adj_queue = nullptr;
   int adj_nsteps = 0, adj_every = 0, adj_nrep = 0;
+  int functional = 0;               // the adjoint's J (mbm_set_functional)
   std::string err;
 };
 
@@ -1689,7 +1690,8 @@ extern "C" int mbm_adjoint_run(mbm_ctx* c, double* t, int nsteps, int every, dou
   double* lam2 = c->adj_buf[1];
   CK(cudaMemsetAsync(c->adj_scal, 0, sizeof(double) * 2, c->stream));
   CK(cudaMemsetAsync(lam, 0, bytes, c->stream));
-  CK(adjoint_functional(c->dblk, c->nblk, c->buf[h.cur], lam, adj_threads(c), c->adj_part, c->adj_scal + 1, c->stream));
+  CK(adjoint_functional(c->dblk, c->nblk, c->buf[h.cur], lam, adj_threads(c), c->adj_part, c->adj_scal + 1,
+                        c->functional, c->stream));
   // reverse sweep over segments [s*every, min((s+1)*every, n)).  The recomputation of
   // segment s-1 from its checkpoint (frozen-dt forward steps, on the low-priority
   // recomputation stream, into the other of the two segment buffers) runs beside the
@@ -1801,6 +1803,7 @@ extern "C" int mbm_replay(mbm_ctx* c, const double* dts, int n, double* J) {
     if (!c->adj_part) CK(cudaMalloc(&c->adj_part, sizeof(double) * ((adj_threads(c) + 127) / 128)));
     CK(cudaMemsetAsync(c->adj_scal, 0, sizeof(double) * 2, c->stream));
     CK(adjoint_functional(c->dblk, c->nblk, c->buf[cur], c->adj_buf[0], adj_threads(c), c->adj_part, c->adj_scal + 1,
+                          c->functional,
                           c->stream));
     double sc[2];
     CK(cudaMemcpyAsync(sc, c->adj_scal, sizeof sc, cudaMemcpyDeviceToHost, c->stream));
@@ -1808,6 +1811,13 @@ extern "C" int mbm_replay(mbm_ctx* c, const double* dts, int n, double* J) {
     *J = sc[1];
   }
   return wait_stream(c);
+}
+
+// the functional J of mbm_adjoint_run and mbm_replay
+extern "C" int mbm_set_functional(mbm_ctx* c, int kind) {
+  if (!c || kind < MBM_J_HEAT_FLUX || kind > MBM_J_DEVIATORIC) return fail(c, MBM_EINVAL, "mbm_set_functional: bad argument");
+  c->functional = kind;
+  return MBM_OK;
 }
 
 // Kn and F of every case (the globals the reference's Steps reads)

@@ -29,12 +29,13 @@ def _theta0(d, rng):
             * rng.uniform(0.5, 1.0) for b in d.blocks]
 
 
-def _fd_check(n, nsteps, every, ndirs, seed, limiter=bf.LIM_AVERAGE, eps=1e-6, Kn=0.01, mode="exact"):
+def _fd_check(n, nsteps, every, ndirs, seed, limiter=bf.LIM_AVERAGE, eps=1e-6, Kn=0.01, mode="exact",
+              functional="heat_flux", with_kn=False):
     d = H.quadrant_deck(n, Kn=Kn, limiter=limiter)
     base = adj.smooth_base(d, seed)
     rng = np.random.default_rng(seed)
     th0 = _theta0(d, rng)
-    with adj.Sensitivity(d, base, mode=mode) as S:
+    with adj.Sensitivity(d, base, mode=mode, functional=functional) as S:
         layers = adj.state_from_theta(d, base, th0)
         S.load(layers)
         J, g, gK, dts, ms = S.run(nsteps, every)
@@ -56,7 +57,22 @@ def _fd_check(n, nsteps, every, ndirs, seed, limiter=bf.LIM_AVERAGE, eps=1e-6, K
         fdK = (Jp - Jm) / (2 * Kn * 1e-6)
         S.load(layers, Kn=Kn)
         assert abs(S.replay(dts) - J) <= 1e-12 * abs(J)      # replay reproduces the forward run
+    if with_kn:
+        return worst, abs(fdK - gK) / abs(fdK), ms, J, fdK, gK
     return worst, abs(fdK - gK) / abs(fdK), ms, J
+
+
+@pytest.mark.parametrize("functional", ["temperature", "deviatoric"])
+def test_adjoint_other_functionals(functional):
+    """The other functionals of mbm_set_functional (the sum of theta, and of the
+    deviatoric temperature tensor's squares) against central differences of the same
+    functional, smooth limiter."""
+    worst, errK, ms, J, fdK, gK = _fd_check(n=24, nsteps=12, every=5, ndirs=6, seed=5,
+                                            functional=functional, with_kn=True)
+    assert J > 0
+    assert worst < 1e-6, worst
+    # dJ/dKn: relative agreement, or absolute where the functional barely depends on Kn
+    assert abs(fdK - gK) <= max(1e-6 * abs(fdK), 1e-9 * abs(J)), (fdK, gK)
 
 
 @pytest.mark.parametrize("limiter", [bf.LIM_NONE, bf.LIM_AVERAGE])
