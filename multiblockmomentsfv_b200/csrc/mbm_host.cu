@@ -505,13 +505,17 @@ static cudaError_t launch_stages(mbm_ctx* c, int heun, int sel_in, int sel_d0, i
   return cudaSuccess;
 }
 
+// programmatic dependent launch for the launches this thread makes while in scope
+struct PdlScope {
+  explicit PdlScope(bool on) { tl_pdl = on; }
+  ~PdlScope() { tl_pdl = false; }
+};
+
 // the body of one step attempt: stage 1, fill TMP, stage 2, fill NEW, controller (the
 // fills inside the stage kernels when they scatter them)
 static cudaError_t launch_attempt(mbm_ctx* c, cudaGraphConditionalHandle h, int use_handle) {
-  struct PdlScope {              // the attempt's launches use it; the thread's others do not
-    explicit PdlScope(bool on) { tl_pdl = on; }
-    ~PdlScope() { tl_pdl = false; }
-  } pdl_scope(c->pdl && c->groups[0].size() <= 1 && c->groups[1].size() <= 1);
+  // the attempt's launches use programmatic dependent launch; the thread's others do not
+  PdlScope pdl_scope(c->pdl && c->groups[0].size() <= 1 && c->groups[1].size() <= 1);
   cudaError_t e;
   const bool g = !c->gscatter;
   if ((e = launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP, 0, nullptr, true))) return e;
@@ -1575,10 +1579,8 @@ static int frozen_step(mbm_ctx* c, const double* in, double* out, const double* 
 // reverse of one step: lam (adjoint of D_{n+1}, interior) -> lam_next (adjoint of
 // D_n); Tn = stage 1 of D_n with its ghost fill
 static int adj_step(mbm_ctx* c, const double* Dn, const double* Tn, double dt, double* lam, double* lam_next) {
-  struct PdlScope {              // the three-pass kernels wait on the device for the one before
-    explicit PdlScope(bool on) { tl_pdl = on; }
-    ~PdlScope() { tl_pdl = false; }
-  } pdl_scope(c->pdl && !c->adj_march);
+  // the three-pass kernels wait on the device for the one before
+  PdlScope pdl_scope(c->pdl && !c->adj_march);
   double* lamT = c->adj_buf[2];
   double* P = c->adj_buf[3];
   const long long nc = adj_threads(c);
