@@ -179,6 +179,53 @@ def test_dirichlet_and_walls_bitwise(oracle_mod):
     assert (t_o, n_o, r_o) == (t_g, n_g, r_g)
 
 
+@pytest.mark.parametrize("limiter", [bf.LIM_AVERAGE, bf.LIM_HARMONIC])
+def test_ffs28_refined_bitwise(oracle_mod, limiter):
+    """The 28-block forward-facing step refined 4 times (28 blocks of 120 x 40 cells:
+    several strips and row segments per block, Dirichlet inflow, walls, 44 interfaces):
+    25 steps equal the oracle's bit for bit, both step loops (graph and host-driven)."""
+    d = bf.parse_file(os.path.join(H.DECKS, "ffs28.txt"), refine=4)
+    d.limiter = limiter
+    scn = sc.Scenario.named("ffs")
+    orc = oracle_mod.Oracle(d, scn)
+    orc.initialise()
+    t_o, n_o, r_o, _ = orc.steps(0.0, 1.0, max_steps=25)
+    for host_loop in ("0", "1"):
+        os.environ["MBM_HOST_LOOP"] = host_loop
+        try:
+            with sv.Solver(d, scn) as s:
+                s.initialise()
+                t_g, n_g, r_g = s.steps(0.0, 1.0, max_steps=25)
+                for b in range(len(d.blocks)):
+                    H.assert_bitwise(s.download(0, b), orc.get_layer(0, b), f"block {b}")
+        finally:
+            del os.environ["MBM_HOST_LOOP"]
+        assert (t_o, n_o, r_o) == (t_g, n_g, r_g)
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_dependent_launch_same_bits(mode):
+    """The step loop with programmatic dependent launch (the default) and without it
+    (MBM_PDL=0) gives the same layers bit for bit."""
+    d = H.quadrant_deck(48, Kn=0.01, limiter=bf.LIM_HARMONIC)
+    scn = sc.Scenario.seeded_quadrant(31)
+    out = {}
+    for pdl in ("1", "0"):
+        os.environ["MBM_PDL"] = pdl
+        try:
+            with sv.Solver(d, scn, mode=mode) as s:
+                s.initialise()
+                res = s.steps(0.0, 1.0, max_steps=40)
+                out[pdl] = (s.dependent_launch(), res, [s.download(l, b) for l in (0, 1, 2)
+                                                        for b in range(len(d.blocks))])
+        finally:
+            del os.environ["MBM_PDL"]
+    assert out["1"][0] and not out["0"][0]
+    assert out["1"][1] == out["0"][1]
+    for a, b in zip(out["1"][2], out["0"][2]):
+        H.assert_bitwise(a, b, "layer")
+
+
 def test_full_size_step_bitwise(oracle_mod):
     """One Heun step (TimeUpdate) of the full benchmark workload (4 blocks x 1024^2,
     seeded quadrant state, Kn = 0.01, harmonic) equals the oracle bit for bit."""
