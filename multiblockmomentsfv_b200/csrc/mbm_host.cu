@@ -43,6 +43,7 @@ cudaError_t launch_control_ext(CaseDev* cases, const BlockDev* blk, unsigned lon
 cudaError_t launch_control(CaseDev* cases, int ncases, const BlockDev* blk, unsigned long long* lam,
                            double* trace, int* queues, cudaGraphConditionalHandle h, int use_handle,
                            cudaStream_t s);
+cudaError_t launch_frozen_prep(CaseDev* cases, const double* ddt, int* queues, cudaStream_t s);
 cudaError_t launch_ckpt(const CaseDev* cases, const double* buf0, const double* buf1, const double* buf2,
                         long long layer_elems, int grid, cudaStream_t s);
 cudaError_t adjoint_stage(const AdjArgs& a0, long long ncell, double* FLx, double* FRx, double* FLy,
@@ -1565,8 +1566,8 @@ static int frozen_begin(mbm_ctx* c) {
 // consecutive steps queue without a host round trip)
 static int frozen_step(mbm_ctx* c, const double* in, double* out, const double* ddt, double* tmp) {
   double* bufs[3] = {const_cast<double*>(in), out, tmp};
-  CK(cudaMemcpyAsync(&c->dcase[0].dt, ddt, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-  CK(cudaMemsetAsync(c->dqueue, 0, sizeof(int) * 10, c->stream));
+  PdlScope pdl_scope(c->pdl && c->groups[0].size() <= 1 && c->groups[1].size() <= 1);
+  CK(launch_frozen_prep(c->dcase, ddt, c->dqueue, c->stream));
   CK(launch_stages(c, 0, SEL_CUR, SEL_CUR, SEL_TMP, 0, bufs, true));
   if (!c->gscatter) CK(launch_ghost(c->dblk, c->dcase, c->dghost, c->nghost, bufs, c->ddir, SEL_TMP, c->stream));
   if (!out) return MBM_OK;

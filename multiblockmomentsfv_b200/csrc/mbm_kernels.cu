@@ -121,6 +121,19 @@ __global__ void control_kernel(CaseDev* cases, int ncases, const BlockDev* __res
   if (use_handle && threadIdx.x == 0) cudaGraphSetConditional(h, live ? 1u : 0u);
 }
 
+// a frozen-dt step's set-up (the adjoint's recomputation, mbm_replay): the step's dt
+// from the device log into the case record, the work counters zeroed -- a kernel, so
+// that the step's launches follow one another as kernels
+__global__ void frozen_prep_kernel(CaseDev* cases, const double* __restrict__ ddt, int* queues) {
+  pdl_enter();
+  if (threadIdx.x == 0) cases[0].dt = *ddt;
+  if (threadIdx.x < 10) queues[threadIdx.x] = 0;
+}
+
+cudaError_t launch_frozen_prep(CaseDev* cases, const double* ddt, int* queues, cudaStream_t s) {
+  return launch_k(frozen_prep_kernel, dim3(1), dim3(32), 0, s, cases, ddt, queues);
+}
+
 // checkpoint of DATA after every ckpt_every-th accepted step (adjoint runs); a
 // rejected attempt copies the same DATA again.  After an accepted step m inside the last
 // segment [a, b) it also keeps that step's stage-1 state (TMP, still the accepted
