@@ -69,7 +69,8 @@ using WarpWindow = typename std::conditional<HEUN == 1, WarpWindow2, WarpWindow1
 // Bulk tensor copies (TMA) of the fast stage 2: one elected lane copies the nine moment
 // planes of 32 columns of one row (a 32 x 1 x 9 box of a 3-D tensor map over a layer of
 // one block: column, row, plane) into a window slot, completing on an mbarrier of the
-// warp; no multicast, the maps cover only this device's layers.  Every wait is bounded.
+// warp; each copy lands in the issuing CTA only, and the maps cover only this device's
+// layers.  Every wait is bounded.
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned long long* bar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
