@@ -158,17 +158,15 @@ __global__ void __launch_bounds__(128, ADJ_FACE_CTAS) adj_faces(AdjArgs a, long 
 // component are issued before any arithmetic; the slope terms of a neighbour are
 // skipped when its slope adjoint is zero (cells no output depends on may hold no
 // state, and 0 * NaN would leak into the sum)
+// one component m of it (the element index i of that component's plane)
 template <int LIM>
-__device__ __forceinline__ void gather_dir(const AdjArgs& a, const BlockDev& B, int I, int J, int dir,
-                                           const double* FL, const double* FR, double* Pb) {
+__device__ __forceinline__ double gather_comp(const AdjArgs& a, const BlockDev& B, int I, int J, int dir,
+                                              const double* FL, const double* FR, long long i) {
   const long long s = dir == 1 ? 1 : B.pitch;
   const int n = dir == 1 ? B.nxp : B.nyp, c = dir == 1 ? I : J;
   const double h = dir == 1 ? B.dx : B.dy, rh = mbm_adj::rcp(h);
-  const long long i0 = cidx(B, I, J);
   const bool lft = c >= 2, rgt = c <= n - 3;      // slopes of c-1 and c+1 exist (off the ring)
-#pragma unroll 1
-  for (int m = 0; m < NV; m++) {
-    const long long i = i0 + m * B.plane;
+  {
     // face (q | q+1) adjoints: FL = its left state, FR = its right state
     const double flm = FL[i - s], fl0 = FL[i], flp = FL[i + s];
     const double frm2 = lft ? FR[i - 2 * s] : 0.0, frm = FR[i - s], fr0 = FR[i];
@@ -195,22 +193,42 @@ __device__ __forceinline__ void gather_dir(const AdjArgs& a, const BlockDev& B, 
       mbm_adj::limit_grad(LIM, pp - p0, pp2 - pp, &g1, &g2);
       g -= lp * g1 * rh;
     }
-    Pb[m] += g;
+    return g;
   }
+}
+
+template <int LIM>
+__device__ __forceinline__ void gather_dir(const AdjArgs& a, const BlockDev& B, int I, int J, int dir,
+                                           const double* FL, const double* FR, double* Pb) {
+  const long long i0 = cidx(B, I, J);
+#pragma unroll 1
+  for (int m = 0; m < NV; m++) Pb[m] += gather_comp<LIM>(a, B, I, J, dir, FL, FR, i0 + m * B.plane);
 }
 
 // pass C: per cell, back to the stage input (and Data0)
 // one cell's share; returns its contribution to dJ/dKn
-template <int HEUN, int LIM>
-__device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, int I, int J, const double* FLx,
-                                           const double* FRx, const double* FLy, const double* FRy) {
-  double Pb[NV] = {0}, Ub[NV] = {0}, U[NV], P0[NV];
+// the adjoint of Data0's relaxation term in the stage-2 update, Conservative(relax(
+// Primitive(D0), -1)) with weight 1/2: adds to *knb, returns the Data0 adjoint in Vb
+__device__ __forceinline__ void data0_adj(const AdjArgs& a, const BlockDev& B, int I, int J, double (&Vb)[NV],
+                                          double* knb) {
+  double Rb[NV], V[NV], W[NV], Q2[NV], C2[NV] = {0}, Pd[NV] = {0};
+#pragma unroll
+  for (int m = 0; m < NV; m++) Rb[m] = 0.5 * a.lout[cidx(B, I, J) + m * B.plane];
+  load9(a.d0, B, I, J, V);
+  mbm_adj::prim(V, W);
+  mbm_adj::relax_p(W, Q2, a.dt, a.Kn, a.F, -1);
+  mbm_adj::cons_adj(Q2, Rb, C2);
+  mbm_adj::relax_p_adj(W, C2, Pd, knb, a.dt, a.Kn, -1);
+  mbm_adj::prim_adj(V, Pd, Vb);
+}
+
+// the rest of a cell's share once its reconstruction and slope adjoints Pb are gathered;
+// D0: the Data0 term here too (stage 2 of the fused cell pass)
+template <int HEUN, bool D0>
+__device__ __forceinline__ double cell_rest(const AdjArgs& a, const BlockDev& B, int I, int J,
+                                            const double (&Pb)[NV]) {
+  double Ub[NV] = {0}, U[NV], P0[NV];
   double knb = 0.0;
-  const bool ring = I == 0 || J == 0 || I == B.nxp - 1 || J == B.nyp - 1;
-  if (!ring) {
-    gather_dir<LIM>(a, B, I, J, 1, FLx, FRx, Pb);
-    gather_dir<LIM>(a, B, I, J, 2, FLy, FRy, Pb);
-  }
   load9(a.x, B, I, J, U);
   mbm_adj::prim(U, P0);
   double Qb[NV] = {0};
@@ -231,15 +249,7 @@ __device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, 
     mbm_adj::relax_p(P0, Q, a.dt, a.Kn, a.F, 2 * HEUN);
     mbm_adj::cons_adj(Q, Rb, Cb);
     mbm_adj::relax_p_adj(P0, Cb, Qb, &knb, a.dt, a.Kn, 2 * HEUN);
-    if (HEUN) {
-      double V[NV], W[NV], Q2[NV], C2[NV] = {0}, Pd[NV] = {0};
-      load9(a.d0, B, I, J, V);
-      mbm_adj::prim(V, W);
-      mbm_adj::relax_p(W, Q2, a.dt, a.Kn, a.F, -1);
-      mbm_adj::cons_adj(Q2, Rb, C2);
-      mbm_adj::relax_p_adj(W, C2, Pd, &knb, a.dt, a.Kn, -1);
-      mbm_adj::prim_adj(V, Pd, Vb);
-    }
+    if (HEUN && D0) data0_adj(a, B, I, J, Vb, &knb);
   }
   bool anyQ = false;
 #pragma unroll
@@ -251,13 +261,25 @@ __device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, 
 #pragma unroll
     for (int m = 0; m < NV; m++) {
       a.lx[ic + m * B.plane] = Ub[m];
-      a.ld0[ic + m * B.plane] = Vb[m];
+      if (D0) a.ld0[ic + m * B.plane] = Vb[m];
     }
   } else if (anyQ) {
 #pragma unroll
     for (int m = 0; m < NV; m++) a.lx[ic + m * B.plane] += Ub[m];
   }
   return knb;
+}
+
+template <int HEUN, int LIM>
+__device__ __forceinline__ double cell_adj(const AdjArgs& a, const BlockDev& B, int I, int J, const double* FLx,
+                                           const double* FRx, const double* FLy, const double* FRy) {
+  double Pb[NV] = {0};
+  const bool ring = I == 0 || J == 0 || I == B.nxp - 1 || J == B.nyp - 1;
+  if (!ring) {
+    gather_dir<LIM>(a, B, I, J, 1, FLx, FRx, Pb);
+    gather_dir<LIM>(a, B, I, J, 2, FLy, FRy, Pb);
+  }
+  return cell_rest<HEUN, true>(a, B, I, J, Pb);
 }
 
 // 64 registers, eight 128-thread CTAs per SM: the pass waits on its neighbour loads, and
@@ -273,6 +295,93 @@ __global__ void __launch_bounds__(128, ADJ_CELL_CTAS) adj_cells(AdjArgs a, long 
   if (k < nthr && locate(a.blk, a.nblk, k, b, I, J))
     knb = cell_adj<HEUN, LIM>(a, a.blk[b], I, J, FLx, FRx, FLy, FRy);
   // the Kn derivative: warp sum, one atomic per warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) knb += __shfl_xor_sync(0xffffffffu, knb, o);
+  if ((threadIdx.x & 31) == 0 && knb != 0.0) atomicAdd(a.knb, knb);
+}
+
+// The cell pass split in two (the default; MBM_ADJ_SPLIT=0 keeps it whole): at 64
+// registers the whole pass kept fifteen nine-vectors live across its stage-2 Data0 term
+// and spilled them (about 80 MB of DRAM writes per launch at 4 x 256^2).  The Data0 term,
+// a function of Data0 and the output adjoint alone, moves to the primitives pass of stage
+// 2; the gather of the reconstruction and slope adjoints (the neighbour loads) stores Pb;
+// a pointwise pass takes it through the relaxation and Primitive.  The same operations
+// in the same order per cell; only dJ/dKn's atomic sums are grouped differently.
+
+// pass A of stage 2 with the Data0 term: the projected primitives as adj_prims, and the
+// Data0 adjoint of every cell (zero off the interior), which starts that adjoint layer
+__global__ void adj_prims_d0(AdjArgs a, long long nthr) {
+  pdl_enter();
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b, I, J;
+  double knb = 0.0;
+  if (k < nthr && locate(a.blk, a.nblk, k, b, I, J)) {
+    const BlockDev B = a.blk[b];
+    double U[NV], P[NV];
+    load9(a.x, B, I, J, U);
+    mbm_adj::prim(U, P);
+    const bool ring = I == 0 || J == 0 || I == B.nxp - 1 || J == B.nyp - 1;
+    if (!ring) {
+      double Q[NV];
+      mbm_adj::relax_p(P, Q, a.dt, a.Kn, a.F, 2 * a.heun + 1);
+#pragma unroll
+      for (int m = 0; m < NV; m++) P[m] = Q[m];
+    }
+    const long long i = cidx(B, I, J);
+#pragma unroll
+    for (int m = 0; m < NV; m++) a.P[i + m * B.plane] = P[m];
+    double Vb[NV] = {0};
+    if (inner(B, I, J)) data0_adj(a, B, I, J, Vb, &knb);
+#pragma unroll
+    for (int m = 0; m < NV; m++) a.ld0[i + m * B.plane] = Vb[m];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) knb += __shfl_xor_sync(0xffffffffu, knb, o);
+  if ((threadIdx.x & 31) == 0 && knb != 0.0) atomicAdd(a.knb, knb);
+}
+
+// pass C1: the reconstruction and slope adjoints Pb of every cell (zero on the ring)
+template <int LIM>
+__global__ void __launch_bounds__(128, ADJ_CELL_CTAS) adj_gather(AdjArgs a, long long nthr, const double* FLx,
+                                                     const double* FRx, const double* FLy, const double* FRy) {
+  pdl_enter();
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b, I, J;
+  if (k >= nthr || !locate(a.blk, a.nblk, k, b, I, J)) return;
+  const BlockDev B = a.blk[b];
+  const bool ring = I == 0 || J == 0 || I == B.nxp - 1 || J == B.nyp - 1;
+  const long long i0 = cidx(B, I, J);
+#pragma unroll 1
+  for (int m = 0; m < NV; m++) {        // (0 + x term) + y term, as the whole pass sums them
+    const long long i = i0 + m * B.plane;
+    double v = 0.0;
+    if (!ring) {
+      v += gather_comp<LIM>(a, B, I, J, 1, FLx, FRx, i);
+      v += gather_comp<LIM>(a, B, I, J, 2, FLy, FRy, i);
+    }
+    a.Pb[i] = v;
+  }
+}
+
+// pass C2: per cell, Pb through the relaxation and Primitive to the stage input, with the
+// update's relaxation term (the Data0 term is in pass A)
+#ifndef ADJ_POINT_CTAS
+#define ADJ_POINT_CTAS 4    // resident 128-thread CTAs per SM the pointwise pass is compiled for
+#endif
+template <int HEUN>
+__global__ void __launch_bounds__(128, ADJ_POINT_CTAS) adj_point(AdjArgs a, long long nthr) {
+  pdl_enter();
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int b, I, J;
+  double knb = 0.0;
+  if (k < nthr && locate(a.blk, a.nblk, k, b, I, J)) {
+    const BlockDev B = a.blk[b];
+    const long long i = cidx(B, I, J);
+    double Pb[NV];
+#pragma unroll
+    for (int m = 0; m < NV; m++) Pb[m] = a.Pb[i + m * B.plane];
+    knb = cell_rest<HEUN, false>(a, B, I, J, Pb);
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) knb += __shfl_xor_sync(0xffffffffu, knb, o);
   if ((threadIdx.x & 31) == 0 && knb != 0.0) atomicAdd(a.knb, knb);
@@ -626,8 +735,14 @@ template <int HEUN, int LIM>
 static void faces_cells(const AdjArgs& a0, long long nthr, unsigned G, double* FLx, double* FRx, double* FLy,
                         double* FRy, cudaStream_t s) {
   launch_k(adj_faces<HEUN, LIM>, dim3(G), dim3(128), 0, s, a0, nthr, FLx, FRx, FLy, FRy);
-  launch_k(adj_cells<HEUN, LIM>, dim3(G), dim3(128), 0, s, a0, nthr, (const double*)FLx, (const double*)FRx,
-           (const double*)FLy, (const double*)FRy);
+  if (a0.Pb) {
+    launch_k(adj_gather<LIM>, dim3(G), dim3(128), 0, s, a0, nthr, (const double*)FLx, (const double*)FRx,
+             (const double*)FLy, (const double*)FRy);
+    launch_k(adj_point<HEUN>, dim3(G), dim3(128), 0, s, a0, nthr);
+  } else {
+    launch_k(adj_cells<HEUN, LIM>, dim3(G), dim3(128), 0, s, a0, nthr, (const double*)FLx, (const double*)FRx,
+             (const double*)FLy, (const double*)FRy);
+  }
 }
 
 template <int HEUN>
@@ -646,7 +761,10 @@ cudaError_t adjoint_stage(const AdjArgs& a0, long long nthr, double* FLx, double
                           double* FRy, cudaStream_t s) {
   const int T = 128;
   const unsigned G = (unsigned)(nthr / T);
-  launch_k(adj_prims, dim3(G), dim3(T), 0, s, a0, nthr);
+  if (a0.Pb && a0.heun)
+    launch_k(adj_prims_d0, dim3(G), dim3(T), 0, s, a0, nthr);
+  else
+    launch_k(adj_prims, dim3(G), dim3(T), 0, s, a0, nthr);
   if (a0.heun) faces_cells_lim<1>(a0, nthr, G, FLx, FRx, FLy, FRy, s);
   else faces_cells_lim<0>(a0, nthr, G, FLx, FRx, FLy, FRy, s);
   return cudaGetLastError();

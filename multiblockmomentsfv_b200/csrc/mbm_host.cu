@@ -152,7 +152,8 @@ struct mbm_ctx {
   double* shard_cfl = nullptr;
   std::vector<int> shard_dir_off, shard_nt;   // Dirichlet rows of every block's edges (whole table)
   // adjoint work space (allocated on first use)
-  double* adj_buf[8] = {nullptr};   // two adjoint layers, stage-1 adjoint, primitives, 4 face-adjoint layers
+  double* adj_buf[9] = {nullptr};   // two adjoint layers, stage-1 adjoint, primitives, 4 face-adjoint layers,
+                                    // the reconstruction adjoint between the two halves of the cell pass
   double* adj_ckpt = nullptr;
   double* adj_seg[2] = {nullptr};    // DATA states of a checkpoint segment (two: recomputation of
   double* adj_segT[2] = {nullptr};   //   the next one beside the reversal of this one); stage-1 states
@@ -1074,7 +1075,7 @@ extern "C" int mbm_destroy(mbm_ctx* c) {
   if (c->hcase) cudaFreeHost(c->hcase);
   cudaFree(c->dlam);
   cudaFree(c->dqueue);
-  for (int k = 0; k < 8; k++) cudaFree(c->adj_buf[k]);
+  for (int k = 0; k < 9; k++) cudaFree(c->adj_buf[k]);
   cudaFree(c->adj_ckpt);
   for (int k = 0; k < 2; k++) {
     cudaFree(c->adj_seg[k]);
@@ -1495,7 +1496,7 @@ static long long adj_threads(mbm_ctx* c) {
 }
 
 static int adj_alloc(mbm_ctx* c, int nsteps, int every) {
-  for (int k = 0; k < 8; k++)      // each one missing (mbm_replay may have made the first)
+  for (int k = 0; k < 9; k++)      // each one missing (mbm_replay may have made the first)
     if (!c->adj_buf[k]) CK(cudaMalloc(&c->adj_buf[k], sizeof(double) * c->layer_elems));
   if (!c->adj_scal) CK(cudaMalloc(&c->adj_scal, sizeof(double) * 2));
   if (!c->adj_part) CK(cudaMalloc(&c->adj_part, sizeof(double) * ((adj_threads(c) + 127) / 128)));
@@ -1584,6 +1585,8 @@ static int adj_step(mbm_ctx* c, const double* Dn, const double* Tn, double dt, d
   PdlScope pdl_scope(c->pdl && !c->adj_march);
   double* lamT = c->adj_buf[2];
   double* P = c->adj_buf[3];
+  const char* se = getenv("MBM_ADJ_SPLIT");     // the cell pass in two halves unless 0
+  double* Pbuf = (se && atoi(se) == 0) ? nullptr : c->adj_buf[8];
   const long long nc = adj_threads(c);
   const CaseDev& h = c->hcase[0];
   // the three-pass cell pass writes every cell of lamT and lam_next in stage 2; the
@@ -1599,6 +1602,7 @@ static int adj_step(mbm_ctx* c, const double* Dn, const double* Tn, double dt, d
   a.blk = c->dblk;
   a.nblk = c->nblk;
   a.P = P;
+  a.Pb = Pbuf;
   a.knb = c->adj_scal;
   a.dt = dt;
   a.Kn = h.Kn;

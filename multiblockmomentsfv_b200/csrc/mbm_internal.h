@@ -128,6 +128,7 @@ struct AdjArgs {       // one stage of the discrete adjoint (mbm_adjoint.cu)
   double* lx;            // += adjoint of the stage input (all cells)
   double* ld0;           // += adjoint of Data0 (stage 2)
   double* P;             // projected primitives of the stage input (layer layout)
+  double* Pb;            // not null: the cell pass split in two, Pb the reconstruction adjoint between them
   double* knb;           // += dJ/dKn
   double dt, Kn, F;
   int limiter, heun;

@@ -350,6 +350,32 @@ def test_tail_segment_kept_by_forward(nsteps, every):
     assert abs(k1 - k0) <= 1e-12 * abs(k0)
 
 
+@pytest.mark.parametrize("limiter", [bf.LIM_AVERAGE, bf.LIM_HARMONIC])
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_split_cell_pass_equals_whole(limiter, mode):
+    """The cell pass in two halves with the Data0 term in the primitives pass (the
+    default) and the whole cell pass (MBM_ADJ_SPLIT=0): the same gradient."""
+    import os
+    d = H.quadrant_deck(40, Kn=0.01, limiter=limiter)
+    base = adj.smooth_base(d, 29)
+    th0 = _theta0(d, np.random.default_rng(29))
+    out = {}
+    for split in ("1", "0"):
+        os.environ["MBM_ADJ_SPLIT"] = split
+        try:
+            with adj.Sensitivity(d, base, mode=mode) as S:
+                S.load(adj.state_from_theta(d, base, th0))
+                J, g, gK, dts, ms = S.run(16, 5)
+                out[split] = (J, np.concatenate([x.ravel() for x in g]), gK)
+        finally:
+            del os.environ["MBM_ADJ_SPLIT"]
+    (J1, g1, k1), (J0, g0, k0) = out["1"], out["0"]
+    assert J1 == J0
+    scale = np.abs(g0).max()
+    assert np.abs(g1 - g0).max() <= 1e-12 * scale, np.abs(g1 - g0).max() / scale
+    assert abs(k1 - k0) <= 1e-12 * abs(k0)
+
+
 def test_replay_before_the_first_adjoint_run():
     """A context whose first call is mbm_replay (which makes only the adjoint layer it
     needs) runs the adjoint afterwards with the same result as a context that runs it
