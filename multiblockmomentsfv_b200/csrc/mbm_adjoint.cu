@@ -366,7 +366,9 @@ __global__ void __launch_bounds__(128, ADJ_CELL_CTAS) adj_gather(AdjArgs a, long
 // pass C2: per cell, Pb through the relaxation and Primitive to the stage input, with the
 // update's relaxation term (the Data0 term is in pass A)
 #ifndef ADJ_POINT_CTAS
-#define ADJ_POINT_CTAS 4    // resident 128-thread CTAs per SM the pointwise pass is compiled for
+// resident 128-thread CTAs per SM the pointwise pass is compiled for: 6 (80 registers, 64
+// bytes of spills) ran the reverse sweep 1 ms faster than 4 (no spills), 5 or 8 (4 x 256^2)
+#define ADJ_POINT_CTAS 6
 #endif
 template <int HEUN>
 __global__ void __launch_bounds__(128, ADJ_POINT_CTAS) adj_point(AdjArgs a, long long nthr) {
